@@ -1,0 +1,387 @@
+#!/usr/bin/env python3
+"""Benchmark of the PRT-LB hot path on B200: D3Q19 TRT flow + ADR transport.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one complete solve of the plain 3D case):
+  64^3 periodic pack of solid spheres, radius U[4, 7], porosity 0.45, seed 0
+  (synthetic stand-in for the reference's rock images);
+  D3Q19 TRT Stokes from rest, float32 populations (f - w, float64 collision,
+  float64 residual), force 2e-6, tau 0.8, run to a relative change of
+  mean |u_x| <= 1e-6 per 50 iterations;
+  then transport of one Monod solute (Ks = 0.5) at Pe = 10, Da = 1 until the
+  reference's stop rule is met (tol 2e-3), 5 snapshots.
+
+value  whole-job GLUPS with inputs resident in HBM: (flow iterations + transport
+       steps) x 64^3 voxels per second, every voxel counted as the reference
+       iterates every voxel; device-timed with CUDA events on the solver's
+       stream, one event pair per step, L2 flushed between steps.
+e2e    the same through the public drop-in API (stokes_d3q19 + solve_adr on
+       host numpy arrays), host<->device copies inside the timed region.
+roofline  the dominant kernel (the D3Q19 stream-collide) against the measured
+       HBM copy bandwidth: algorithmic bytes = 152 B per pore voxel (19
+       float32 read + written) + 1 B mask per voxel, per iteration.
+cpu_baseline  the NumPy oracle (a restatement of the reference's algorithm)
+       on a bounded sample of the same workload, one core.
+
+--impl reference times the reference's CPU algorithm (the oracle port, since
+the reference is Python that does not travel to the GPU host) with one
+process per host core, on the same metric.
+
+Multi-GPU: replicas only (the path does not shard; one independent solve per
+rank), value = all ranks' updates / max-over-ranks time.
+"""
+
+import argparse
+import contextlib
+import ctypes
+import io
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "prt-deeponet-gui_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+EDGE = 64
+POROSITY = 0.45
+SEED = 0
+FORCE, TAU, FLOW_TOL, FLOW_NIT = 2e-6, 0.8, 1e-6, 30000
+PE, DA, KS, N_T = 10.0, 1.0, 0.5, 5
+METRIC = "D3Q19 TRT+ADR GLUPS"
+UNIT = "GLUPS"
+LB_BYTES_PER_FLUID = 19 * 4 * 2  # float32 populations read + written
+WORKLOAD = ("plain-3d: 64^3 sphere pack (r U[4,7], porosity 0.45, seed 0), D3Q19 TRT fp32 "
+            "to tol 1e-6 + Monod ADR (Ks 0.5) Pe 10 Da 1 to the stop rule")
+
+
+def geometry():
+    from prtlb_gpu.geometry import sphere_pack_3d
+    return sphere_pack_3d(EDGE, POROSITY, SEED)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks(object):
+    """nvidia-smi sampled every 200 ms while the timed region runs."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % os.getpid())
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 7:
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def flush_l2(torch, dev):
+    buf = flush_l2.buf
+    if buf is None:
+        buf = flush_l2.buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    buf.fill_(1)
+
+
+flush_l2.buf = None
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def device_solve(ctx, L, d_mat, d_vel, d_out, shape, chem):
+    """One complete solve on device-resident buffers; returns (iters, steps)."""
+    from prtlb_gpu import _lib
+    from prtlb_gpu.adr import prepare, stats_dict, _run_device
+    p = _lib.FlowParams()
+    p.nd = 3
+    for i in range(3):
+        p.dims[i] = shape[i]
+    p.nit, p.force, p.tau, p.magic, p.tol = FLOW_NIT, FORCE, TAU, 3.0 / 16.0, FLOW_TOL
+    p.every, p.precision = 50, _lib.PRT_FP32
+    fi = _lib.FlowInfo()
+    ctx.check(L.prt_flow_dev(ctx.handle, ctypes.c_void_p(d_mat), ctypes.byref(p),
+                             ctypes.c_void_p(d_vel), ctypes.byref(fi)))
+    geom = _lib.AdrGeom()
+    geom.nd = 3
+    for i in range(3):
+        geom.dims[i] = shape[i]
+    geom.pore_code, geom.biofilm_code = 2, -1
+    st = _lib.AdrStats()
+    ctx.check(L.prt_adr_stage_dev(ctx.handle, ctypes.c_void_p(d_mat), ctypes.c_void_p(d_vel),
+                                  ctypes.byref(geom), ctypes.byref(st)))
+    S = prepare(shape, stats_dict(st), PE, DA, n_species=1, chem=chem)
+    steps = _run_device(ctx, S, N_T, d_out)
+    return int(fi.iters), int(steps)
+
+
+def run_ours(args, rank, world, torch, dist):
+    from prtlb_gpu import _lib, solve_adr, stokes_d3q19
+    from prtlb_gpu.chemistry import monod_chemistry
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    g = geometry()
+    shape = g.shape
+    ncell = int(np.prod(shape))
+    nfluid = int((g == 2).sum())
+    chem = monod_chemistry(KS)
+    ctx = _lib.Context(dev)
+    L = _lib.lib()
+    t_mat = torch.from_numpy(g.copy()).to(f"cuda:{dev}")
+    t_vel = torch.empty((3,) + shape, dtype=torch.float32, device=f"cuda:{dev}")
+    t_out = torch.empty((N_T, 1) + shape, dtype=torch.float32, device=f"cuda:{dev}")
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=f"cuda:{dev}")
+
+    def step():
+        return device_solve(ctx, L, t_mat.data_ptr(), t_vel.data_ptr(), t_out.data_ptr(), shape,
+                            chem)
+
+    quiet = contextlib.redirect_stdout(io.StringIO())
+    with quiet:
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches()
+    ms_steps, flow_ms, adr_ms, iters, nsteps = [], [], [], [], []
+    with Clocks(dev) as clk, contextlib.redirect_stdout(io.StringIO()):
+        for _ in range(args.steps):
+            flush_l2(torch, f"cuda:{dev}")
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            it, ns = step()
+            e1.record(stream)
+            e1.synchronize()
+            ms_steps.append(e0.elapsed_time(e1))
+            tm = ctx.timing()
+            flow_ms.append(tm[0])
+            adr_ms.append(tm[2])
+            iters.append(it)
+            nsteps.append(ns)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    launches = ctx.launches() - launches0
+    total_ms = float(sum(ms_steps))
+    updates = float(sum(iters) + sum(nsteps)) * ncell
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = updates * world / (total_ms * 1e-3) / 1e9
+
+    # e2e: the drop-in API on host arrays
+    e2e_ms = []
+    h2d = d2h = 0
+    with contextlib.redirect_stdout(io.StringIO()):
+        for k in range(max(1, min(args.steps, 3))):
+            flush_l2(torch, f"cuda:{dev}")
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            v = stokes_d3q19(g, nit=FLOW_NIT, force=FORCE, tau_lb=TAU, tol=FLOW_TOL,
+                             precision="fp32", ctx=ctx)
+            out, tn = solve_adr(g, v, pe=PE, da=DA, n_t=N_T, n_species=1, chem=chem, ctx=ctx)
+            e1.record(stream)
+            e1.synchronize()
+            e2e_ms.append(e0.elapsed_time(e1))
+    h2d = g.nbytes + g.nbytes + v.nbytes           # flow: mat; transport: mat + vel
+    d2h = v.nbytes + out.nbytes                    # flow: vel; transport: snapshots
+    e2e_updates = float(iters[0] + nsteps[0]) * ncell
+    e2e_value = e2e_updates * world / (statistics.mean(e2e_ms) * 1e-3) / 1e9
+
+    # roofline of the dominant kernel from this run's own events
+    fl_ms = statistics.mean(flow_ms)
+    ad_ms = statistics.mean(adr_ms)
+    per_launch_ms = fl_ms / max(iters[0], 1)
+    lb_bytes = nfluid * LB_BYTES_PER_FLUID + ncell
+    achieved = lb_bytes / (per_launch_ms * 1e-3) / 1e9
+    peak, kind = peaks()
+    roof = {"kernel": "lb_step_kernel<D3Q19,float,double>", "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": kind,
+            "bytes_per_launch": lb_bytes, "traffic": None,
+            "note": "per-launch time = flow loop events / iterations (includes graph "
+                    "launch gaps and the convergence check); 64^3 state (20 MB) is L2-resident"}
+    res = {"ms_per_step": total_ms / args.steps, "value": value, "e2e": e2e_value,
+           "h2d": h2d, "d2h": d2h, "launches": launches, "roof": roof, "clocks": clk.summary(),
+           "flow_ms": fl_ms, "adr_ms": ad_ms, "iters": iters[0], "adr_steps": nsteps[0],
+           "ncell": ncell, "nfluid": nfluid}
+    ctx.close()
+    return res
+
+
+# ---------------------------------------------------------------------------
+# CPU: the oracle (a restatement of the reference's NumPy algorithm)
+# ---------------------------------------------------------------------------
+def cpu_sample(args_tuple):
+    """Time a bounded sample of the workload with the NumPy oracle:
+    `its` flow iterations and `steps` transport steps on the 64^3 pack."""
+    its, steps = args_tuple
+    sys.path[:0] = [ROOT, PKG]
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    from oracle import prtlb_oracle as O
+    from prtlb_gpu.chemistry import monod_chemistry
+    g = geometry()
+    t0 = time.perf_counter()
+    v = O.stokes(g, nit=its, force=FORCE, tau_lb=TAU, tol=0.0)
+    t1 = time.perf_counter()
+    v[0] += 1e-4 * (g == 2)  # a moving field for the transport sample
+    with contextlib.redirect_stdout(io.StringIO()):
+        O.solve_adr(g, v, pe=PE, da=DA, n_t=2, n_species=1, steps=steps,
+                    chem=monod_chemistry(KS))
+    t2 = time.perf_counter()
+    n = g.size
+    return {"flow_s": t1 - t0, "adr_s": t2 - t1, "updates": float(its + steps) * n,
+            "its": its, "steps": steps}
+
+
+def cpu_baseline_line(procs, its, steps):
+    ctxm = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    if procs == 1:
+        res = [cpu_sample((its, steps))]
+    else:
+        with ctxm.Pool(procs) as pool:
+            res = pool.map(cpu_sample, [(its, steps)] * procs)
+    wall = time.perf_counter() - t0
+    per = [r["updates"] / (r["flow_s"] + r["adr_s"]) for r in res]
+    value = sum(per) / 1e9
+    return value, res, wall
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-its", type=int, default=20)
+    ap.add_argument("--cpu-steps", type=int, default=100)
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    config = {"workload": WORKLOAD, "edge": EDGE, "voxels": EDGE ** 3, "porosity": POROSITY,
+              "seed": SEED, "flow": "D3Q19 TRT fp32 (f-w), fp64 collide+residual",
+              "transport": "Monod Ks 0.5, Pe 10, Da 1, n_t 5, stop rule tol 2e-3",
+              "l2": "flushed (256 MB write) before every timed step",
+              "parallelism": "replicas" if world > 1 else "single"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        procs = os.cpu_count() or 1
+        vals = []
+        for _ in range(args.warmup + args.steps):
+            v, res, wall = cpu_baseline_line(procs, 4, 20)
+            vals.append(v)
+        value = statistics.median(vals[args.warmup:]) if args.steps else vals[-1]
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config,
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port",
+                                 "sample": "per process: 4 D3Q19 iterations + 20 transport "
+                                           "steps of the 64^3 workload (NumPy oracle)"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_mod
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+    r = run_ours(args, rank, world, torch, dist)
+    if rank == 0:
+        cpu = None
+        if world == 1:
+            v, res, wall = cpu_baseline_line(1, args.cpu_its, args.cpu_steps)
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": "%d D3Q19 iterations + %d Monod transport steps of the 64^3 "
+                             "workload, NumPy oracle, %.1f s" % (args.cpu_its, args.cpu_steps,
+                                                                 wall)}
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "config": config,
+                "e2e": {"value": r["e2e"], "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
+                        "d2h_bytes_per_step": r["d2h"]},
+                "gpu_launches": r["launches"], "roofline": r["roof"], "clocks": r["clocks"],
+                "cpu_baseline": cpu,
+                "detail": {"flow_ms": r["flow_ms"], "transport_ms": r["adr_ms"],
+                           "flow_iters": r["iters"], "transport_steps": r["adr_steps"],
+                           "voxels": r["ncell"], "pore_voxels": r["nfluid"],
+                           "solves_per_hour": 3.6e6 / r["ms_per_step"] * world}}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,260 @@
+/*
+ * prtlb.h -- C ABI of the B200 PRT-LB solver (libprtlb.so).
+ *
+ * The reference (PRT-LB, a pure NumPy simulator) has no native interface; its
+ * callers import three Python functions by name:
+ *
+ *   stokes_d2q9   3D/tools/prtlb_2d.py:348   D2Q9 TRT Stokes flow
+ *   stokes_d3q19  3D/tools/prtlb_3d.py:348   D3Q19 TRT Stokes flow
+ *   solve_adr     3D/tools/prtlb_3d.py:781   finite-volume ADR + reactions
+ *                 (byte-identical copy at 3D/tools/prtlb_2d.py:812)
+ *
+ * Every entry point below is what a ctypes binding of those functions binds.
+ * The Python package prtlb_gpu wraps them with the reference's signatures.
+ *
+ * Conventions
+ *   - Plain C types only.  Host pointers are borrowed for the duration of the
+ *     call; device memory is owned by the context.
+ *   - Every call returns PRT_OK (0) or a negative status; prt_last_error()
+ *     gives the message.  No C++ exception crosses this boundary.
+ *   - One context = one CUDA device + one stream.  Calls on one context are
+ *     serialised by the caller; different contexts may run concurrently.
+ *   - Grids are C-ordered material arrays: (nx, ny) in 2D, (nx, ny, nz) in 3D,
+ *     material code 2 = pore (the reference's PORE, prtlb_3d.py SOLID/WALL/PORE).
+ */
+#ifndef PRTLB_H
+#define PRTLB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PRT_ABI_VERSION 1
+#define PRT_MAX_SPECIES 8
+
+/* status codes */
+#define PRT_OK 0
+#define PRT_E_INVALID (-1)   /* bad argument (the reference raises ValueError) */
+#define PRT_E_CUDA (-2)      /* a CUDA call failed */
+#define PRT_E_OOM (-3)       /* device allocation failed */
+#define PRT_E_STATE (-4)     /* call made out of order (e.g. run before begin) */
+#define PRT_E_CANCELLED (-5) /* the progress callback asked to stop */
+#define PRT_E_NODEV (-6)     /* no CUDA device */
+
+/* population storage for the flow solve */
+#define PRT_FP64 0 /* float64, as the reference                            */
+#define PRT_FP32 1 /* float32 holding f_i - w_i, collided in float64        */
+#define PRT_FP16 2 /* float16 holding (f_i - w_i) * 2^k, collided in float32 */
+
+typedef struct prt_ctx prt_ctx;
+
+/* ABI version of the loaded library (PRT_ABI_VERSION at build time). */
+int prt_abi_version(void);
+
+/* Create a context on CUDA device `device`.  *out is NULL on failure. */
+int prt_create(int device, prt_ctx** out);
+
+/* Release every device buffer of the context and the context itself. */
+void prt_destroy(prt_ctx* ctx);
+
+/* Message of the last failed call on ctx (ctx == NULL: last prt_create). */
+const char* prt_last_error(const prt_ctx* ctx);
+
+/* Number of kernels this context has launched so far (graph nodes included). */
+int64_t prt_kernel_launches(const prt_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order or time
+ * their own work around the solver's. */
+void* prt_stream(const prt_ctx* ctx);
+
+/* Device time of the last solve's time loops, from CUDA events recorded on
+ * the context's stream around them: out[0] flow loop ms, out[1] its
+ * iterations, out[2] transport loop ms, out[3] its steps. */
+int prt_last_timing(const prt_ctx* ctx, double* out4);
+
+/* sizeof of the ABI structs, for binding checks (needs no GPU):
+ * 0 prt_flow_params, 1 prt_flow_info, 2 prt_adr_params,
+ * 3 prt_adr_run_params, 4 prt_adr_result, 5 prt_adr_geom,
+ * 6 prt_adr_stats; anything else: 0. */
+size_t prt_sizeof(int which);
+
+/* ------------------------------------------------------------------------ */
+/* Flow: stokes_d2q9 / stokes_d3q19                                         */
+/* ------------------------------------------------------------------------ */
+
+/* Arguments of stokes_d3q19(g, nit, force, tau_lb, magic, tol, info)
+ * (prtlb_3d.py:348) and stokes_d2q9 (prtlb_2d.py:348). */
+typedef struct prt_flow_params {
+    int32_t nd;        /* 2 (D2Q9) or 3 (D3Q19) */
+    int32_t dims[3];   /* nx, ny, nz (nz ignored when nd == 2) */
+    int64_t nit;       /* iteration CAP, FlowConvergence max_it */
+    double force;      /* body force along +x, lattice units */
+    double tau;        /* relaxation time, > 0.5 */
+    double magic;      /* TRT magic parameter Lambda (3/16) */
+    double tol;        /* stop when the relative change of mean|u_x| per
+                          `every` iterations is <= tol; tol <= 0: never */
+    int32_t every;     /* convergence check interval (50), must be even */
+    int32_t precision; /* PRT_FP64 / PRT_FP32 / PRT_FP16 */
+} prt_flow_params;
+
+/* What the solve reports (FlowConvergence.report, prtlb_3d.py:237, plus the
+ * FP64 reductions the reference does not have). */
+typedef struct prt_flow_info {
+    int64_t iters;         /* flow_iters */
+    int32_t converged;     /* flow_converged */
+    int32_t pad0;
+    double change;         /* flow_change (inf when never evaluated) */
+    int64_t fluid_cells;   /* pore voxels */
+    int64_t nonfinite;     /* non-finite float32 velocity components */
+    double umax;           /* max float32 speed over pore voxels */
+    double speed_sum;      /* FP64 sum of float32 speed over pore voxels */
+    double ux_sum;         /* FP64 sum of u_x over pore voxels (pre-cast) */
+    double mass;           /* FP64 sum of rho over pore voxels */
+    double permeability;   /* nu * <u_x>_V / force, voxel^2, <>_V over ALL cells */
+    double fp16_scale;     /* 2^k scale used by PRT_FP16 (1 otherwise) */
+} prt_flow_info;
+
+/* Host buffers: mat (nx*ny[*nz] uint8), vel_out (3*nx*ny[*nz] float32,
+ * component-major, zero in solid; in 2D vel_out[2] == 0). */
+int prt_flow(prt_ctx* ctx, const uint8_t* mat, const prt_flow_params* p,
+             float* vel_out, prt_flow_info* info);
+
+/* Same, with DEVICE pointers (already resident on the context's device). */
+int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p,
+                 float* d_vel_out, prt_flow_info* info);
+
+/* ------------------------------------------------------------------------ */
+/* Transport: solve_adr (prtlb_3d.py:781-1595)                              */
+/* ------------------------------------------------------------------------ */
+
+/* Everything the time loop needs, already reduced to float32 lattice numbers
+ * by the host exactly as solve_adr's set-up computes them (9.1-9.3). */
+typedef struct prt_adr_params {
+    int32_t nd;
+    int32_t dims[3];
+    int32_t ns;                 /* chemicals */
+    uint32_t moving_mask;       /* bit j: chemical j is transported */
+    uint32_t pinned_mask;       /* bit j: moving and fed (inlet not NaN) */
+    int32_t pore_code;          /* 2 */
+    int32_t biofilm_code;       /* material code of biofilm voxels, -1: none */
+    float u_scale;              /* float32 velocity scale (mean axial or speed) */
+    float dt;                   /* float32 time step */
+    float feed[PRT_MAX_SPECIES];
+    /* initial condition: 0 zero, 1 every solute voxel, 2 biofilm voxels only */
+    int32_t init_mode[PRT_MAX_SPECIES];
+    float init_value[PRT_MAX_SPECIES];
+    /* harmonic face diffusivities, float32: [pore|pore, pore|biofilm, biofilm|biofilm] */
+    float dface[PRT_MAX_SPECIES][3];
+    /* biotic dual-Monod (rate_biotic, prtlb_3d.py:1224) */
+    int32_t biotic_on;
+    float k;                    /* Da / l_ref */
+    int32_t ks_donor_pos;       /* ks_donor > 0 */
+    float ks_donor;
+    int32_t ks_acceptor_pos;    /* ks_acceptor > 0 */
+    float ks_acceptor;
+    int32_t coupled;            /* biomass_coupled and ns > 3 and c_init[3] > 0 */
+    float c3_init;
+    float neg_alpha;            /* float32(-alpha) */
+    int32_t alpha_cap;          /* ns > 1 and alpha > 0 */
+    float alpha_dt;             /* float32(float32(alpha) * dt) */
+    float prod_coef;            /* float32(1 - (yield if ns > 3 else 0)) */
+    float yield_;               /* float32(yield) */
+    float kd;                   /* biomass decay, lattice */
+    /* abiotic first order (rate_abiotic, prtlb_3d.py:1271) */
+    int32_t abio_on;            /* ka > 0 and abiotic_index < ns */
+    int32_t j_ab;               /* abiotic_index */
+    int32_t j_mk;               /* abiotic_product_index, -1: none */
+    float ka;
+    int32_t surface_only;
+    /* reversible sorption (new term, no reference counterpart):
+       r = k_sorp * (C[j_c] - C[j_s] / K_d), dC[j_c] -= r, dC[j_s] += r */
+    int32_t sorp_on;
+    int32_t j_c;
+    int32_t j_s;
+    float k_sorp;
+    float inv_kd_sorp;
+    int32_t pad1;
+} prt_adr_params;
+
+/* Progress callback: solve_adr's on_progress(step, limit, mean, change).
+ * Return non-zero to cancel the run (PRT_E_CANCELLED). */
+typedef int (*prt_progress_cb)(void* user, int64_t step, int64_t limit,
+                               double mean0, double change);
+
+typedef struct prt_adr_run_params {
+    int64_t limit;        /* steps if given, else max_steps */
+    int32_t until_conv;   /* 1: steps is None (stop rule active) */
+    int32_t check;        /* max(int(1/dt), 100) */
+    double tol;           /* solve_adr tol */
+    double ratio;         /* snapshot ladder ratio (1.12) */
+} prt_adr_run_params;
+
+typedef struct prt_adr_result {
+    int64_t steps;        /* n at exit */
+    int32_t hit_cap;      /* until_conv and n >= limit */
+    int32_t ladder;       /* snapshots kept (len(keep_steps)) */
+    int64_t checks;       /* convergence checks evaluated */
+    double last_rest;     /* rest of the last check (inf if none) */
+} prt_adr_result;
+
+/* Which voxels hold solute: pore, plus biofilm when a biofilm code is set
+ * (solve_adr 9.1, prtlb_3d.py:831-846). */
+typedef struct prt_adr_geom {
+    int32_t nd;
+    int32_t dims[3];
+    int32_t pore_code;    /* 2 */
+    int32_t biofilm_code; /* -1: none */
+} prt_adr_geom;
+
+/* What solve_adr's set-up reads from the velocity field, over the solute
+ * voxels m, in float32 with numpy's summation order (prtlb_3d.py:860-865,
+ * 977-978): vel[0][m].mean(), sqrt(sum_a vel[a]^2)[m].mean(), max |vel[a]|. */
+typedef struct prt_adr_stats {
+    int64_t solute_voxels;
+    int64_t biofilm_voxels;
+    float mean_axial;
+    float mean_speed;
+    float vmax[3];
+    float pad;
+} prt_adr_stats;
+
+/* Stage 1 of a transport solve: take the material grid and the flow field
+ * (float32, (3, grid) component-major as stokes_* returns), build the voxel
+ * flags and the summation tree, and return the velocity statistics the host
+ * needs to derive the time step.  Host buffers are copied; device buffers
+ * are borrowed until prt_adr_begin returns. */
+int prt_adr_stage(prt_ctx* ctx, const uint8_t* mat, const float* vel,
+                  const prt_adr_geom* geom, prt_adr_stats* stats);
+int prt_adr_stage_dev(prt_ctx* ctx, const uint8_t* d_mat, const float* d_vel,
+                      const prt_adr_geom* geom, prt_adr_stats* stats);
+
+/* Stage 2: with the lattice numbers, build the face velocities, the initial
+ * state and ladder snapshot 0.  The geometry must match the staged one. */
+int prt_adr_begin(prt_ctx* ctx, const prt_adr_params* p);
+
+/* Run the time loop.  cb may be NULL. */
+int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progress_cb cb,
+                void* user, prt_adr_result* res);
+
+/* Ladder step numbers (keep_steps), count written to *count. */
+int prt_adr_ladder(prt_ctx* ctx, int64_t* steps, int32_t cap, int32_t* count);
+
+/* Copy ladder snapshot `slot` ((ns, grid) float32) to host / device memory. */
+int prt_adr_fetch(prt_ctx* ctx, int32_t slot, float* out);
+int prt_adr_fetch_dev(prt_ctx* ctx, int32_t slot, float* d_out);
+
+/* Per-species float32 pore means of snapshot `slot`, computed with numpy's
+ * float32 pairwise summation order (what solve_adr's check uses). */
+int prt_adr_means(prt_ctx* ctx, int32_t slot, float* means);
+
+/* Release the transport state of the context. */
+int prt_adr_end(prt_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRTLB_H */

@@ -1,0 +1,733 @@
+// adr.cu -- the transport step of PRT-LB (solve_adr, prtlb_3d.py:781-1595)
+// for sm_100a: finite-volume advection (MUSCL/minmod), harmonic-mean
+// diffusion, the C div(u) correction, the inlet Dirichlet feed, the reaction
+// source terms, forward Euler and the clip, fused into one launch per step.
+//
+// This file is compiled with -fmad=false.  The reference integrates in
+// float32 with numpy, one rounding per operation; with no fused multiply-add
+// and the reference's operation order kept below, every voxel of every step
+// is bit-identical to it, and so are the convergence means (numpy's float32
+// pairwise summation is replayed by adr_means_*), the stop step and the
+// snapshots.
+#include "prt_internal.h"
+
+namespace prt {
+
+// numpy's elementwise semantics ---------------------------------------------
+__device__ __forceinline__ float np_min(float a, float b) { return (a <= b || a != a) ? a : b; }
+__device__ __forceinline__ float np_max(float a, float b) { return (a >= b || a != a) ? a : b; }
+__device__ __forceinline__ float np_sign(float a) {
+    return a > 0.f ? 1.f : (a < 0.f ? -1.f : (a != a ? a : 0.f));
+}
+
+// _muscl (prtlb_3d.py:650-705): up + 1/2 minmod(down - up, up - upup), the
+// minmod written as 1/2 (sgn a + sgn b) min(|a|, |b|).
+__device__ __forceinline__ float muscl(float up, float upup, float down) {
+    const float d1 = down - up;
+    const float d2 = up - upup;
+    const float slope = (0.5f * (np_sign(d1) + np_sign(d2))) * np_min(fabsf(d1), fabsf(d2));
+    return up + 0.5f * slope;
+}
+
+template <int ND>
+struct Axes;
+template <>
+struct Axes<3> {
+    static constexpr int n = 3;
+    __host__ __device__ static constexpr int ax(int i) { return i; }
+};
+template <>
+struct Axes<2> {  // a 2D grid (nx, ny) is stored as (nx, 1, ny)
+    static constexpr int n = 2;
+    __host__ __device__ static constexpr int ax(int i) { return i == 0 ? 0 : 2; }
+};
+
+struct VoxelPos {
+    int p[3];
+    long long c;
+};
+
+__device__ __forceinline__ VoxelPos voxel_pos(long long c, const Grid& g) {
+    VoxelPos v;
+    v.c = c;
+    unsigned long long t = (unsigned long long)c;
+    v.p[2] = (int)(t % (unsigned)g.nz);
+    t /= (unsigned)g.nz;
+    v.p[1] = (int)(t % (unsigned)g.ny);
+    v.p[0] = (int)(t / (unsigned)g.ny);
+    return v;
+}
+
+__device__ __forceinline__ int extent(const Grid& g, int a) {
+    return a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
+}
+__device__ __forceinline__ long long stride(const Grid& g, int a) {
+    return a == 0 ? (long long)g.ny * g.nz : (a == 1 ? (long long)g.nz : 1ll);
+}
+// index of the low face of voxel v along axis a in the (n_a + 1)-long face array
+__device__ __forceinline__ long long face_lo(const Grid& g, const VoxelPos& v, int a) {
+    if (a == 0) return v.c;
+    if (a == 1) return ((long long)v.p[0] * (g.ny + 1) + v.p[1]) * g.nz + v.p[2];
+    return ((long long)v.p[0] * g.ny + v.p[1]) * (g.nz + 1) + v.p[2];
+}
+__device__ __forceinline__ long long face_step(const Grid& g, int a) {
+    return a == 0 ? (long long)g.ny * g.nz : (a == 1 ? (long long)g.nz : 1ll);
+}
+
+// A neighbour value of chemical j.  Every neighbour that is actually read is a
+// solute voxel (the open / far flags guarantee it), so it is on the inlet
+// plane exactly when its x is 0; there the pinned feed replaces the stored
+// value (step(), prtlb_3d.py:1392-1400, pins before transport).
+__device__ __forceinline__ float ld_c(const float* __restrict__ Cj, long long c, int x, bool pin,
+                                      float feed) {
+    return (pin && x == 0) ? feed : Cj[c];
+}
+
+// transport() of one chemical at one voxel (prtlb_3d.py:1182-1208).
+template <int ND>
+__device__ __forceinline__ float transport_one(const float* __restrict__ Cj, const Grid& g,
+                                               const VoxelPos& v, uint32_t fl,
+                                               const float* const* __restrict__ face, float Cc,
+                                               bool pin, float feed, const float (&dj)[3]) {
+    float out = 0.f;
+    float divu = 0.f;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+        const int a = Axes<ND>::ax(i);
+        const int p = v.p[a];
+        const int n = extent(g, a);
+        const long long s = stride(g, a);
+        const bool oL = fl & f_open_lo(a), oH = fl & f_open_hi(a);
+        const bool fL = fl & f_far_lo(a), fH = fl & f_far_hi(a);
+        // clamped (edge-replicated) neighbour positions
+        const int pm1 = p > 0 ? p - 1 : 0, pm2 = p > 1 ? p - 2 : 0;
+        const int pp1 = p < n - 1 ? p + 1 : n - 1, pp2 = p < n - 2 ? p + 2 : n - 1;
+        const int x0 = v.p[0];
+        const int xm1 = (a == 0) ? pm1 : x0, xm2 = (a == 0) ? pm2 : x0;
+        const int xp1 = (a == 0) ? pp1 : x0, xp2 = (a == 0) ? pp2 : x0;
+        const float Cm1 = oL ? ld_c(Cj, v.c + (long long)(pm1 - p) * s, xm1, pin, feed) : Cc;
+        const float Cp1 = oH ? ld_c(Cj, v.c + (long long)(pp1 - p) * s, xp1, pin, feed) : Cc;
+        const float Cm2 = fL ? ld_c(Cj, v.c + (long long)(pm2 - p) * s, xm2, pin, feed) : Cm1;
+        const float Cp2 = fH ? ld_c(Cj, v.c + (long long)(pp2 - p) * s, xp2, pin, feed) : Cp1;
+        const long long fi = face_lo(g, v, a);
+        const float uL = face[a][fi];
+        const float uH = face[a][fi + face_step(g, a)];
+        const int bf = (fl & F_BF) ? 1 : 0;
+        const float DL = oL ? dj[bf + ((fl & f_nbf_lo(a)) ? 1 : 0)] : 0.f;
+        const float DH = oH ? dj[bf + ((fl & f_nbf_hi(a)) ? 1 : 0)] : 0.f;
+        // out += D_hi (C+1 - C) + D_lo (C-1 - C)
+        out = out + (DH * (Cp1 - Cc) + DL * (Cm1 - Cc));
+        const float fh = (uH >= 0.f) ? muscl(Cc, Cm1, Cp1) : muscl(Cp1, Cp2, Cc);
+        const float flo = (uL >= 0.f) ? muscl(Cm1, Cm2, Cc) : muscl(Cc, Cp1, Cm1);
+        // out -= u_hi f_hi - u_lo f_lo
+        out = out - (uH * fh - uL * flo);
+        divu = divu + (uH - uL);
+    }
+    return out + Cc * divu;
+}
+
+// The reaction terms (rate_biotic, rate_abiotic, reaction: prtlb_3d.py:1224-1367)
+// at one voxel, plus the reversible-sorption exchange (no reference counterpart).
+template <int NS>
+__device__ __forceinline__ void reaction(const float (&C)[NS], float surf,
+                                         const prt_adr_params& p, float (&dC)[NS]) {
+#pragma unroll
+    for (int j = 0; j < NS; ++j) dC[j] = 0.f;
+    float R = 0.f;
+    if (p.biotic_on) {
+        R = p.ks_donor_pos ? (p.k * C[0]) / (p.ks_donor + C[0]) : p.k * C[0];
+        if (NS > 1) R = R * (p.ks_acceptor_pos ? C[NS > 1 ? 1 : 0] / (p.ks_acceptor + C[NS > 1 ? 1 : 0])
+                                               : C[NS > 1 ? 1 : 0]);
+        if (NS > 3 && p.coupled) R = (R * C[NS > 3 ? 3 : 0]) / p.c3_init;
+        // caps: R <= 1/2 min(C0 / dt, C1 / (alpha dt))
+        float lim = C[0] / p.dt;
+        if (NS > 1 && p.alpha_cap) lim = np_min(lim, C[NS > 1 ? 1 : 0] / p.alpha_dt);
+        R = np_min(R, 0.5f * lim);
+    }
+    float Ra = 0.f;
+    if (p.abio_on) {
+        float cj = 0.f;
+#pragma unroll
+        for (int j = 0; j < NS; ++j)
+            if (j == p.j_ab) cj = C[j];
+        Ra = p.surface_only ? (p.ka * cj) * surf : p.ka * cj;
+        Ra = np_min(Ra, (0.5f * cj) / p.dt);
+    }
+    if (p.biotic_on) {
+        dC[0] = -R;
+        if (NS > 1) dC[NS > 1 ? 1 : 0] = p.neg_alpha * R;
+        if (NS > 2) dC[NS > 2 ? 2 : 0] = p.prod_coef * R;
+        if (NS > 3) dC[NS > 3 ? 3 : 0] = p.yield_ * R - p.kd * C[NS > 3 ? 3 : 0];
+    } else {
+        // R is the float32 scalar 0: -R, -alpha R, coef R are zeros, biomass 0
+    }
+    if (p.abio_on) {
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            if (j == p.j_ab) dC[j] = dC[j] - Ra;
+        }
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            if (j == p.j_mk && p.j_mk != p.j_ab) dC[j] = dC[j] + Ra;
+        }
+    }
+    if (p.sorp_on) {
+        float c = 0.f, s = 0.f;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            if (j == p.j_c) c = C[j];
+            if (j == p.j_s) s = C[j];
+        }
+        float r = p.k_sorp * (c - s * p.inv_kd_sorp);
+        r = np_min(r, (0.5f * c) / p.dt);
+        r = np_max(r, -((0.5f * s) / p.dt));
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            if (j == p.j_c) dC[j] = dC[j] - r;
+            if (j == p.j_s) dC[j] = dC[j] + r;
+        }
+    }
+}
+
+constexpr int kAdrThreads = 256;
+
+// One transport step n = n_base + kstep + 1: reads the state after step n-1
+// from buf[(n-1)&1], writes the state after step n to buf[n&1] and, when n is
+// a snapshot step, also to its ladder slot.
+template <int ND, int NS>
+__global__ void __launch_bounds__(kAdrThreads) adr_step_kernel(AdrDev d, prt_adr_params p,
+                                                               const AdrCtrl* __restrict__ ctrl,
+                                                               int kstep) {
+    const long long n = ctrl->n_base + kstep + 1;
+    if (ctrl->done || n > ctrl->limit) return;  // uniform over the grid
+    const long long c = (long long)blockIdx.x * kAdrThreads + threadIdx.x;
+    if (c >= d.g.n) return;
+    const uint32_t fl = d.flags[c];
+    if (!(fl & F_M)) return;  // rock: stays 0 in every buffer
+    const long long N = d.g.n;
+    const float* __restrict__ Cin = d.buf[(n - 1) & 1];
+    float* __restrict__ Cout = d.buf[n & 1];
+    const VoxelPos v = voxel_pos(c, d.g);
+    const bool x0 = fl & F_X0;
+    float C[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        const bool pin = (p.pinned_mask >> j) & 1u;
+        C[j] = (pin && x0) ? p.feed[j] : Cin[(long long)j * N + c];
+    }
+    float T[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        T[j] = 0.f;
+        if ((p.moving_mask >> j) & 1u) {
+            const bool pin = (p.pinned_mask >> j) & 1u;
+            const float dj[3] = {p.dface[j][0], p.dface[j][1], p.dface[j][2]};
+            T[j] = transport_one<ND>(Cin + (long long)j * N, d.g, v, fl, d.face, C[j], pin,
+                                     p.feed[j], dj);
+        }
+    }
+    float surf = 0.f;
+    if (p.abio_on && p.surface_only) {
+        float nface = 0.f;
+#pragma unroll
+        for (int i = 0; i < ND; ++i) {
+            const int a = Axes<ND>::ax(i);
+            nface = nface + ((fl & f_open_lo(a)) ? 0.f : 1.f);
+            nface = nface + ((fl & f_open_hi(a)) ? 0.f : 1.f);
+        }
+        surf = nface / (float)(2 * ND);
+    }
+    float dC[NS];
+    reaction<NS>(C, surf, p, dC);
+    const int slot = d.slot_of_step[n];
+    float* __restrict__ lad = slot >= 0 ? d.ladder + (long long)slot * NS * N : nullptr;
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        const bool mv = (p.moving_mask >> j) & 1u;
+        const float rhs = mv ? (T[j] + dC[j]) : dC[j];
+        float cn = C[j] + p.dt * rhs;
+        cn = np_max(cn, 0.f);
+        Cout[(long long)j * N + c] = cn;
+        if (lad) lad[(long long)j * N + c] = cn;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// set-up (solve_adr 9.1-9.8, prtlb_3d.py:831-1158, 1425-1440)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool is_m(const uint8_t* mat, long long c, int pore, int bf) {
+    const int v = mat[c];
+    return v == pore || (bf >= 0 && v == bf);
+}
+__device__ __forceinline__ bool is_bf(const uint8_t* mat, long long c, int bf) {
+    return bf >= 0 && mat[c] == bf;
+}
+
+__global__ void adr_flags_kernel(const uint8_t* __restrict__ mat, Grid g, int nd, int pore,
+                                 int bfc, uint32_t* __restrict__ flags, uint8_t* __restrict__ mflag) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.n) return;
+    const VoxelPos v = voxel_pos(c, g);
+    const bool m = is_m(mat, c, pore, bfc);
+    uint32_t fl = 0;
+    if (m) fl |= F_M;
+    if (is_bf(mat, c, bfc)) fl |= F_BF;
+    if (m && v.p[0] == 0) fl |= F_X0;
+    for (int i = 0; i < nd; ++i) {
+        const int a = (nd == 3) ? i : (i == 0 ? 0 : 2);
+        const int p = v.p[a];
+        const int n = extent(g, a);
+        const long long s = stride(g, a);
+        const int pm1 = p > 0 ? p - 1 : 0, pm2 = p > 1 ? p - 2 : 0;
+        const int pp1 = p < n - 1 ? p + 1 : n - 1, pp2 = p < n - 2 ? p + 2 : n - 1;
+        const long long cm1 = c + (long long)(pm1 - p) * s, cm2 = c + (long long)(pm2 - p) * s;
+        const long long cp1 = c + (long long)(pp1 - p) * s, cp2 = c + (long long)(pp2 - p) * s;
+        const bool oL = m && is_m(mat, cm1, pore, bfc);
+        const bool oH = m && is_m(mat, cp1, pore, bfc);
+        const bool fL = oL && is_m(mat, cm2, pore, bfc);
+        const bool fH = oH && is_m(mat, cp2, pore, bfc);
+        if (oL) fl |= f_open_lo(a);
+        if (oH) fl |= f_open_hi(a);
+        if (fL) fl |= f_far_lo(a);
+        if (fH) fl |= f_far_hi(a);
+        if (is_bf(mat, cm1, bfc)) fl |= f_nbf_lo(a);
+        if (is_bf(mat, cp1, bfc)) fl |= f_nbf_hi(a);
+    }
+    flags[c] = fl;
+    mflag[c] = m ? 1 : 0;
+}
+
+// Face velocities u_f = 1/2 (u_lo + u_hi) on open faces, 0 on closed ones,
+// from u = vel / u_scale (float32 division) masked to the solute voxels
+// (prtlb_3d.py:860-865, 1092-1135).  Face f of axis a lies between voxels
+// clamp(f-1) and clamp(f); faces 0 and n_a are the domain faces.
+__global__ void adr_faces_kernel(const uint8_t* __restrict__ mat, const float* __restrict__ vcomp,
+                                 Grid g, int a, int pore, int bfc, float u_scale,
+                                 float* __restrict__ face) {
+    const int fa = extent(g, a) + 1;
+    const long long nf = g.n / extent(g, a) * fa;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nf) return;
+    int q[3];
+    const int dims[3] = {a == 0 ? fa : g.nx, a == 1 ? fa : g.ny, a == 2 ? fa : g.nz};
+    unsigned long long r = (unsigned long long)t;
+    q[2] = (int)(r % (unsigned)dims[2]);
+    r /= (unsigned)dims[2];
+    q[1] = (int)(r % (unsigned)dims[1]);
+    q[0] = (int)(r / (unsigned)dims[1]);
+    const int f = q[a];
+    const int n = extent(g, a);
+    const int plo = f - 1 < 0 ? 0 : f - 1;
+    const int phi = f > n - 1 ? n - 1 : f;
+    int ql[3] = {q[0], q[1], q[2]}, qh[3] = {q[0], q[1], q[2]};
+    ql[a] = plo;
+    qh[a] = phi;
+    const long long cl = ((long long)ql[0] * g.ny + ql[1]) * g.nz + ql[2];
+    const long long ch = ((long long)qh[0] * g.ny + qh[1]) * g.nz + qh[2];
+    const bool ml = is_m(mat, cl, pore, bfc), mh = is_m(mat, ch, pore, bfc);
+    float u = 0.f;
+    if (ml && mh) {
+        const float ul = vcomp[cl] / u_scale;
+        const float uh = vcomp[ch] / u_scale;
+        u = 0.5f * (ul + uh);
+    }
+    face[t] = u;
+}
+
+// Initial state (initial(), prtlb_3d.py:1425-1440) into buffer 0 and slot 0.
+__global__ void adr_init_kernel(const uint32_t* __restrict__ flags, Grid g, prt_adr_params p,
+                                float* __restrict__ buf0, float* __restrict__ slot0) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.n) return;
+    const uint32_t fl = flags[c];
+    for (int j = 0; j < p.ns; ++j) {
+        float v = 0.f;
+        if (p.init_mode[j] == 1 && (fl & F_M)) v = p.init_value[j];
+        if (p.init_mode[j] == 2 && (fl & F_BF)) v = p.init_value[j];
+        buf0[(long long)j * g.n + c] = v;
+        if (slot0) slot0[(long long)j * g.n + c] = v;
+    }
+}
+
+// Order-preserving compaction of the solute voxels (C order), in three passes.
+constexpr int kScanBlock = 1024;
+__global__ void count_kernel(const uint8_t* __restrict__ mflag, long long n, int* __restrict__ cnt) {
+    const long long c = (long long)blockIdx.x * kScanBlock + threadIdx.x;
+    int v = (c < n && mflag[c]) ? 1 : 0;
+    v = __syncthreads_count(v);
+    if (threadIdx.x == 0) cnt[blockIdx.x] = v;
+}
+__global__ void scan_counts_kernel(int* __restrict__ cnt, int nb, long long* __restrict__ total) {
+    // one thread: the block counts are few (n / 1024)
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    long long acc = 0;
+    for (int i = 0; i < nb; ++i) {
+        const int v = cnt[i];
+        cnt[i] = (int)acc;
+        acc += v;
+    }
+    *total = acc;
+}
+__global__ void scatter_kernel(const uint8_t* __restrict__ mflag, long long n,
+                               const int* __restrict__ off, int* __restrict__ idx) {
+    __shared__ int warp_tot[kScanBlock / 32];
+    const long long c = (long long)blockIdx.x * kScanBlock + threadIdx.x;
+    const int v = (c < n && mflag[c]) ? 1 : 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int before = __popc(bal & ((1u << lane) - 1u));
+    if (lane == 0) warp_tot[w] = __popc(bal);
+    __syncthreads();
+    int base = 0;
+    for (int i = 0; i < w; ++i) base += warp_tot[i];
+    if (v) idx[off[blockIdx.x] + base + before] = (int)c;
+}
+
+// ---------------------------------------------------------------------------
+// numpy float32 pairwise means (the stop rule's `C[j][m].mean()`)
+// ---------------------------------------------------------------------------
+__global__ void means_leaf_kernel(const float* __restrict__ src, long long N,
+                                  const int* __restrict__ idx, PairTree t, int ns,
+                                  float* __restrict__ vals) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long long)t.nleaf * ns) return;
+    const int leaf = (int)(tid % t.nleaf);
+    const int j = (int)(tid / t.nleaf);
+    const float* s = src + (long long)j * N;
+    const int* ix = idx + t.leaf_start[leaf];
+    const int len = t.leaf_len[leaf];
+    float res;
+    if (len < 8) {
+        res = 0.f;
+        for (int i = 0; i < len; ++i) res = res + s[ix[i]];
+    } else {
+        float r0 = s[ix[0]], r1 = s[ix[1]], r2 = s[ix[2]], r3 = s[ix[3]];
+        float r4 = s[ix[4]], r5 = s[ix[5]], r6 = s[ix[6]], r7 = s[ix[7]];
+        int i = 8;
+        for (; i < len - (len % 8); i += 8) {
+            r0 = r0 + s[ix[i + 0]];
+            r1 = r1 + s[ix[i + 1]];
+            r2 = r2 + s[ix[i + 2]];
+            r3 = r3 + s[ix[i + 3]];
+            r4 = r4 + s[ix[i + 4]];
+            r5 = r5 + s[ix[i + 5]];
+            r6 = r6 + s[ix[i + 6]];
+            r7 = r7 + s[ix[i + 7]];
+        }
+        res = ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7));
+        for (; i < len; ++i) res = res + s[ix[i]];
+    }
+    vals[(long long)j * (t.nleaf + t.ninner) + leaf] = res;
+}
+
+__global__ void means_tree_kernel(PairTree t, long long nm, float* __restrict__ vals,
+                                  float* __restrict__ means) {
+    const int j = blockIdx.x;
+    float* v = vals + (long long)j * (t.nleaf + t.ninner);
+    for (int h = 0; h < t.nlevel; ++h) {
+        for (int i = t.level_off[h] + threadIdx.x; i < t.level_off[h + 1]; i += blockDim.x)
+            v[t.nleaf + i] = v[t.inner_l[i]] + v[t.inner_r[i]];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float sum = t.root >= 0 ? 0.f + v[t.root] : 0.f;
+        means[j] = sum / (float)nm;  // 0/0 -> NaN for an empty pore space, as numpy
+    }
+}
+
+// The check of the time loop (prtlb_3d.py:1499-1543), in float64 like the
+// reference's arrays of Python floats.
+__device__ __forceinline__ double npd_max(double a, double b) { return (a >= b || a != a) ? a : b; }
+
+__global__ void adr_stop_kernel(AdrCtrl* ctrl, const float* __restrict__ means, ProgressRec* log,
+                                int log_cap, cudaGraphConditionalHandle h, int use_handle) {
+    if (threadIdx.x != 0) return;
+    if (ctrl->done) {
+        if (use_handle) cudaGraphSetConditional(h, 0);
+        return;
+    }
+    const long long base = ctrl->n_base;
+    const long long end = min(base + (long long)ctrl->check, ctrl->limit);
+    if (end > base && end % ctrl->check == 0) {
+        const int ns = ctrl->ns;
+        double cur[PRT_MAX_SPECIES], stepc[PRT_MAX_SPECIES];
+        double change = 0.0, rest = 0.0;
+        bool first = true;
+        for (int j = 0; j < ns; ++j) {
+            cur[j] = (double)means[j];
+            ctrl->scale[j] = npd_max(ctrl->scale[j], fabs(cur[j]));
+            stepc[j] = fabs(cur[j] - ctrl->prev[j]) / ctrl->scale[j];
+            const double r = ctrl->prev_change[j] > 0 ? stepc[j] / ctrl->prev_change[j] : 0.0;
+            double rj = (r < 1.0) ? stepc[j] * r / npd_max(1.0 - r, 1e-12) : INFINITY;
+            if (!isfinite(rj)) rj = INFINITY;
+            if (first) {
+                change = stepc[j];
+                rest = rj;
+                first = false;
+            } else {
+                change = (change != change) ? change : ((stepc[j] != stepc[j]) ? stepc[j] : fmax(change, stepc[j]));
+                rest = fmax(rest, rj);
+            }
+        }
+        if (ctrl->nlog < log_cap) {
+            ProgressRec& rec = log[ctrl->nlog];
+            rec.n = end;
+            rec.mean0 = cur[0];
+            rec.value = isfinite(rest) ? rest : change;
+        }
+        ctrl->nlog += 1;
+        ctrl->checks += 1;
+        ctrl->last_rest = rest;
+        if (ctrl->until_conv && end >= 10ll * ctrl->check && rest <= ctrl->tol) {
+            ctrl->converged = 1;
+            ctrl->done = 1;
+        } else {
+            for (int j = 0; j < ns; ++j) {
+                ctrl->prev[j] = cur[j];
+                ctrl->prev_change[j] = stepc[j];
+            }
+        }
+    }
+    ctrl->n_base = end;
+    if (end >= ctrl->limit) ctrl->done = 1;
+    const int go = (!ctrl->done && end < ctrl->n_pause) ? 1 : 0;
+    if (use_handle) cudaGraphSetConditional(h, go);
+}
+
+__global__ void adr_means_pick_kernel(const AdrCtrl* ctrl, const float* buf0, const float* buf1,
+                                      const float** out) {
+    // chooses the buffer holding the state at the end of the current chunk
+    const long long end = min(ctrl->n_base + (long long)ctrl->check, ctrl->limit);
+    *out = (end & 1) ? buf1 : buf0;
+}
+
+// means over the buffer the device picked (graph body: pointer comes from device memory)
+__global__ void means_leaf_indirect_kernel(const AdrCtrl* __restrict__ ctrl, const float* const* src_p,
+                                           long long N, const int* __restrict__ idx, PairTree t,
+                                           int ns, float* __restrict__ vals) {
+    if (ctrl->done) return;
+    const long long base = ctrl->n_base;
+    const long long end = min(base + (long long)ctrl->check, ctrl->limit);
+    if (!(end > base && end % ctrl->check == 0)) return;
+    const float* src = *src_p;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (long long)t.nleaf * ns) return;
+    const int leaf = (int)(tid % t.nleaf);
+    const int j = (int)(tid / t.nleaf);
+    const float* s = src + (long long)j * N;
+    const int* ix = idx + t.leaf_start[leaf];
+    const int len = t.leaf_len[leaf];
+    float res;
+    if (len < 8) {
+        res = 0.f;
+        for (int i = 0; i < len; ++i) res = res + s[ix[i]];
+    } else {
+        float r0 = s[ix[0]], r1 = s[ix[1]], r2 = s[ix[2]], r3 = s[ix[3]];
+        float r4 = s[ix[4]], r5 = s[ix[5]], r6 = s[ix[6]], r7 = s[ix[7]];
+        int i = 8;
+        for (; i < len - (len % 8); i += 8) {
+            r0 = r0 + s[ix[i + 0]];
+            r1 = r1 + s[ix[i + 1]];
+            r2 = r2 + s[ix[i + 2]];
+            r3 = r3 + s[ix[i + 3]];
+            r4 = r4 + s[ix[i + 4]];
+            r5 = r5 + s[ix[i + 5]];
+            r6 = r6 + s[ix[i + 6]];
+            r7 = r7 + s[ix[i + 7]];
+        }
+        res = ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7));
+        for (; i < len; ++i) res = res + s[ix[i]];
+    }
+    vals[(long long)j * (t.nleaf + t.ninner) + leaf] = res;
+}
+
+__global__ void means_tree_cond_kernel(const AdrCtrl* __restrict__ ctrl, PairTree t, long long nm,
+                                       float* __restrict__ vals, float* __restrict__ means) {
+    if (ctrl->done) return;
+    const long long base = ctrl->n_base;
+    const long long end = min(base + (long long)ctrl->check, ctrl->limit);
+    if (!(end > base && end % ctrl->check == 0)) return;
+    const int j = blockIdx.x;
+    float* v = vals + (long long)j * (t.nleaf + t.ninner);
+    for (int h = 0; h < t.nlevel; ++h) {
+        for (int i = t.level_off[h] + threadIdx.x; i < t.level_off[h + 1]; i += blockDim.x)
+            v[t.nleaf + i] = v[t.inner_l[i]] + v[t.inner_r[i]];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float sum = t.root >= 0 ? 0.f + v[t.root] : 0.f;
+        means[j] = sum / (float)nm;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <int ND, int NS>
+static cudaError_t step_t(const AdrDev& d, const prt_adr_params& p, AdrCtrl* ctrl, int k,
+                          cudaStream_t s) {
+    const unsigned nb = (unsigned)((d.g.n + kAdrThreads - 1) / kAdrThreads);
+    adr_step_kernel<ND, NS><<<nb, kAdrThreads, 0, s>>>(d, p, ctrl, k);
+    return cudaGetLastError();
+}
+
+template <int ND>
+static cudaError_t step_nd(const AdrDev& d, const prt_adr_params& p, AdrCtrl* ctrl, int k,
+                           cudaStream_t s) {
+    switch (d.ns) {
+        case 1: return step_t<ND, 1>(d, p, ctrl, k, s);
+        case 2: return step_t<ND, 2>(d, p, ctrl, k, s);
+        case 3: return step_t<ND, 3>(d, p, ctrl, k, s);
+        case 4: return step_t<ND, 4>(d, p, ctrl, k, s);
+        case 5: return step_t<ND, 5>(d, p, ctrl, k, s);
+        case 6: return step_t<ND, 6>(d, p, ctrl, k, s);
+        case 7: return step_t<ND, 7>(d, p, ctrl, k, s);
+        case 8: return step_t<ND, 8>(d, p, ctrl, k, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t adr_launch_step(const AdrDev& d, const prt_adr_params& p, AdrCtrl* ctrl, int kstep,
+                            cudaStream_t s) {
+    return d.nd == 3 ? step_nd<3>(d, p, ctrl, kstep, s) : step_nd<2>(d, p, ctrl, kstep, s);
+}
+
+// float32 speed sqrt((v0^2 + v1^2) [+ v2^2]) the way numpy forms it
+__global__ void speed_kernel(const float* __restrict__ vel, Grid g, int nd,
+                             float* __restrict__ sp) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.n) return;
+    const float v0 = vel[c];
+    const float v1 = vel[g.n + c];
+    float s = v0 * v0 + v1 * v1;
+    if (nd == 3) {
+        const float v2 = vel[2 * g.n + c];
+        s = s + v2 * v2;
+    }
+    sp[c] = sqrtf(s);
+}
+
+// max |vel[a]| over the solute voxels (order-free: max is exact)
+__global__ void vmax_kernel(const float* __restrict__ vel, const int* __restrict__ idx, long long nm,
+                            long long n, int nd, unsigned* __restrict__ out) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    float m[3] = {0.f, 0.f, 0.f};
+    if (t < nm) {
+        const long long c = idx[t];
+        for (int a = 0; a < nd; ++a) m[a] = fabsf(vel[(long long)a * n + c]);
+    }
+    for (int a = 0; a < 3; ++a) {
+        float v = m[a];
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0 && v > 0.f) atomicMax(out + a, __float_as_uint(v));
+    }
+}
+
+__global__ void count_bf_kernel(const uint32_t* __restrict__ flags, long long n,
+                                unsigned long long* out) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int v = (c < n && (flags[c] & F_BF)) ? 1 : 0;
+    v = __syncthreads_count(v);
+    if (threadIdx.x == 0 && v) atomicAdd(out, (unsigned long long)v);
+}
+
+cudaError_t adr_launch_flags(const uint8_t* mat, const Grid& g, int nd, int pore, int bfc,
+                             uint32_t* flags, uint8_t* mflag, cudaStream_t s) {
+    const unsigned nb = (unsigned)((g.n + 255) / 256);
+    adr_flags_kernel<<<nb, 256, 0, s>>>(mat, g, nd, pore, bfc, flags, mflag);
+    return cudaGetLastError();
+}
+
+// mean_axial, mean_speed (numpy float32 pairwise means over the solute
+// voxels) into means[0..1]; max |v_a| bits into vmax_bits[0..2]; biofilm
+// voxel count into *nbf.  tmp: n floats of scratch.
+cudaError_t adr_launch_vel_stats(const float* vel, const AdrDev& d, float* tmp, float* means,
+                                 unsigned* vmax_bits, unsigned long long* nbf, cudaStream_t s) {
+    const Grid& g = d.g;
+    const unsigned nb = (unsigned)((g.n + 255) / 256);
+    cudaError_t e;
+    for (int which = 0; which < 2; ++which) {
+        const float* src = vel;
+        if (which == 1) {
+            speed_kernel<<<nb, 256, 0, s>>>(vel, g, d.nd, tmp);
+            src = tmp;
+        }
+        if (d.tree.nleaf > 0) {
+            means_leaf_kernel<<<(unsigned)((d.tree.nleaf + 255) / 256), 256, 0, s>>>(
+                src, g.n, d.idx, d.tree, 1, d.tree_vals);
+        }
+        means_tree_kernel<<<1, 256, 0, s>>>(d.tree, d.nm, d.tree_vals, means + which);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (d.nm > 0)
+        vmax_kernel<<<(unsigned)((d.nm + 255) / 256), 256, 0, s>>>(vel, d.idx, d.nm, g.n, d.nd,
+                                                                  vmax_bits);
+    count_bf_kernel<<<nb, 256, 0, s>>>(d.flags, g.n, nbf);
+    return cudaGetLastError();
+}
+
+// Face velocities and the initial state; the flags are already built.
+cudaError_t adr_launch_setup(const uint8_t* mat, const float* vel, const prt_adr_params& p,
+                             const AdrDev& d, cudaStream_t s) {
+    const Grid& g = d.g;
+    const unsigned nb = (unsigned)((g.n + 255) / 256);
+    cudaError_t e;
+    for (int i = 0; i < d.nd; ++i) {
+        const int a = (d.nd == 3) ? i : (i == 0 ? 0 : 2);
+        const int ext = a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
+        const long long nf = g.n / ext * (ext + 1);
+        // velocity component of storage axis a: 3D -> a; 2D -> x: 0, y (stored as z): 1
+        const int comp = (d.nd == 3) ? a : (a == 0 ? 0 : 1);
+        adr_faces_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(
+            mat, vel + (long long)comp * g.n, g, a, p.pore_code, p.biofilm_code, p.u_scale,
+            const_cast<float*>(d.face[a]));
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    adr_init_kernel<<<nb, 256, 0, s>>>(d.flags, g, p, d.buf[0], d.ladder);
+    return cudaGetLastError();
+}
+
+cudaError_t adr_launch_compact(const uint8_t* mflag, long long n, int* cnt, long long* total,
+                               int* idx, cudaStream_t s) {
+    const int nb = (int)((n + kScanBlock - 1) / kScanBlock);
+    count_kernel<<<nb, kScanBlock, 0, s>>>(mflag, n, cnt);
+    scan_counts_kernel<<<1, 32, 0, s>>>(cnt, nb, total);
+    if (idx) scatter_kernel<<<nb, kScanBlock, 0, s>>>(mflag, n, cnt, idx);
+    return cudaGetLastError();
+}
+
+cudaError_t adr_launch_means(const AdrDev& d, AdrCtrl* ctrl, int slot, float* means_out,
+                             cudaStream_t s) {
+    // explicit means of ladder slot `slot` (slot >= 0), outside the time loop
+    (void)ctrl;
+    const float* src = d.ladder + (long long)slot * d.ns * d.g.n;
+    if (d.tree.nleaf > 0) {
+        const long long nt = (long long)d.tree.nleaf * d.ns;
+        means_leaf_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(src, d.g.n, d.idx, d.tree, d.ns,
+                                                                       d.tree_vals);
+    }
+    means_tree_kernel<<<d.ns, 256, 0, s>>>(d.tree, d.nm, d.tree_vals, means_out);
+    return cudaGetLastError();
+}
+
+cudaError_t adr_launch_chunk_means(const AdrDev& d, AdrCtrl* ctrl, const float** src_slot,
+                                   float* means_out, cudaStream_t s) {
+    adr_means_pick_kernel<<<1, 1, 0, s>>>(ctrl, d.buf[0], d.buf[1], src_slot);
+    if (d.tree.nleaf > 0) {
+        const long long nt = (long long)d.tree.nleaf * d.ns;
+        means_leaf_indirect_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(
+            ctrl, src_slot, d.g.n, d.idx, d.tree, d.ns, d.tree_vals);
+    }
+    means_tree_cond_kernel<<<d.ns, 256, 0, s>>>(ctrl, d.tree, d.nm, d.tree_vals, means_out);
+    return cudaGetLastError();
+}
+
+cudaError_t adr_launch_stop(const AdrDev& d, AdrCtrl* ctrl, const float* means,
+                            cudaGraphConditionalHandle h, int use_handle, cudaStream_t s) {
+    adr_stop_kernel<<<1, 32, 0, s>>>(ctrl, means, d.log, d.log_cap, h, use_handle);
+    return cudaGetLastError();
+}
+
+}  // namespace prt

@@ -1,0 +1,147 @@
+// prt_internal.h -- structures shared by the kernel translation units and the
+// host runtime of libprtlb.so.  Not part of the public ABI (include/prtlb.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/prtlb.h"
+
+namespace prt {
+
+// A grid in the storage frame.  3D (nx, ny, nz) is kept as is; a 2D (nx, ny)
+// grid is stored as (nx, 1, ny) so that the contiguous axis is always the
+// last one and the linear index (x*ny + y) is unchanged.
+struct Grid {
+    int nx, ny, nz;
+    long long n;  // nx*ny*nz
+};
+
+// Device-side state of FlowConvergence (prtlb_3d.py:168-252) for one solve.
+struct FlowCtrl {
+    long long it_base;  // iterations completed before the current chunk
+    long long nit;      // cap
+    long long iters;    // flow_iters
+    long long nfluid;
+    double tol;
+    double prev;
+    double change;
+    int every;
+    int done;
+    int has_prev;
+    int converged;
+};
+
+template <class R>
+struct LbConst {
+    R omp, omm;   // omega+ , omega-
+    R half_g;     // force / 2, added to the x momentum
+    R guo[9];     // w_a (1 - omega-/2) 3 g c_ax for the first member of each pair
+    float scale;  // FP16 storage scale (2^k) and its inverse
+    float inv_scale;
+};
+
+// Control block of one transport solve (the while loop of prtlb_3d.py:1493).
+struct AdrCtrl {
+    long long n_base;  // steps completed before the current chunk
+    long long limit;
+    long long n_pause;  // host asked to regain control at this step
+    long long checks;
+    int check;
+    int until_conv;
+    int done;
+    int converged;
+    int ns;
+    int nlog;
+    double tol;
+    double last_rest;
+    double prev[PRT_MAX_SPECIES];
+    double prev_change[PRT_MAX_SPECIES];
+    double scale[PRT_MAX_SPECIES];
+};
+
+struct ProgressRec {
+    long long n;
+    double mean0;
+    double value;
+};
+
+// Flag bits of one transport voxel (built once per solve by adr_setup).
+enum : uint32_t {
+    F_M = 1u << 0,        // solute voxel (pore or biofilm)
+    F_BF = 1u << 1,       // biofilm voxel
+    F_X0 = 1u << 2,       // on the x = 0 face (the inlet plane)
+    // per axis a (0..2): open_lo, open_hi, far_lo, far_hi at 3 + 4a
+    F_AX0 = 3,
+    // biofilm neighbour lo/hi per axis a at 15 + 2a
+    F_NBF0 = 15,
+};
+
+__host__ __device__ inline uint32_t f_open_lo(int a) { return 1u << (F_AX0 + 4 * a + 0); }
+__host__ __device__ inline uint32_t f_open_hi(int a) { return 1u << (F_AX0 + 4 * a + 1); }
+__host__ __device__ inline uint32_t f_far_lo(int a) { return 1u << (F_AX0 + 4 * a + 2); }
+__host__ __device__ inline uint32_t f_far_hi(int a) { return 1u << (F_AX0 + 4 * a + 3); }
+__host__ __device__ inline uint32_t f_nbf_lo(int a) { return 1u << (F_NBF0 + 2 * a + 0); }
+__host__ __device__ inline uint32_t f_nbf_hi(int a) { return 1u << (F_NBF0 + 2 * a + 1); }
+
+// numpy's float32 pairwise summation tree over the solute voxels, flattened:
+// leaves [0, nleaf) sum runs of <= 128 consecutive compressed values, internal
+// nodes [nleaf, nleaf + ninner) add two earlier values; inner nodes are sorted
+// by height so each height is one parallel level.
+struct PairTree {
+    int nleaf;
+    int ninner;
+    int nlevel;
+    int root;             // value index of the root (-1 when there are no voxels)
+    const int* leaf_start;
+    const int* leaf_len;
+    const int* inner_l;
+    const int* inner_r;
+    const int* level_off;  // nlevel + 1 offsets into the inner arrays
+};
+
+// Kernel launchers (flow.cu) ------------------------------------------------
+// Returns cudaSuccess or the launch error.
+cudaError_t flow_launch_step(int nd, int precision, bool odd, bool check, void* f,
+                             const uint8_t* fluid, const Grid& g, const void* lbconst,
+                             const FlowCtrl* ctrl, int kstep, double* partials,
+                             cudaStream_t s);
+cudaError_t flow_launch_check(FlowCtrl* ctrl, const double* partials, int nblocks,
+                              cudaGraphConditionalHandle h, int use_handle, cudaStream_t s);
+cudaError_t flow_launch_moments(int nd, int precision, bool odd, const void* f,
+                                const uint8_t* fluid, const Grid& g, const void* lbconst,
+                                float* vel, double* partials, cudaStream_t s);
+cudaError_t flow_launch_fluid_mask(const uint8_t* mat, uint8_t* fluid, long long n,
+                                   int pore_code, cudaStream_t s);
+cudaError_t flow_launch_final_reduce(const double* partials, int nblocks, double* out,
+                                     cudaStream_t s);
+int flow_blocks(const Grid& g);
+
+// Kernel launchers (adr.cu) -------------------------------------------------
+struct AdrDev {
+    Grid g;
+    int nd;
+    int ns;
+    const uint32_t* flags;
+    const float* face[3];
+    float* buf[2];
+    float* ladder;              // slot s at ladder + s * ns * n
+    const int* slot_of_step;    // -1 or ladder slot for step n
+    const int* idx;             // compressed solute voxel list
+    long long nm;               // solute voxels
+    PairTree tree;
+    float* tree_vals;           // ns * (nleaf + ninner)
+    ProgressRec* log;
+    int log_cap;
+};
+
+cudaError_t adr_launch_setup(const uint8_t* mat, const float* vel, const prt_adr_params& p,
+                             const AdrDev& d, cudaStream_t s);
+cudaError_t adr_launch_step(const AdrDev& d, const prt_adr_params& p, AdrCtrl* ctrl,
+                            int kstep, cudaStream_t s);
+cudaError_t adr_launch_means(const AdrDev& d, AdrCtrl* ctrl, int slot_or_neg, float* means_out,
+                             cudaStream_t s);
+cudaError_t adr_launch_stop(const AdrDev& d, AdrCtrl* ctrl, const float* means,
+                            cudaGraphConditionalHandle h, int use_handle, cudaStream_t s);
+
+}  // namespace prt

@@ -1,0 +1,944 @@
+// runtime.cu -- the C ABI of libprtlb.so (include/prtlb.h): contexts, device
+// buffers, and the two time loops run as CUDA graphs with a device-side
+// while-condition, so a whole flow solve or transport solve is one graph
+// launch and the host waits once.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "prt_internal.h"
+
+using namespace prt;
+
+namespace prt {
+cudaError_t adr_launch_compact(const uint8_t* mflag, long long n, int* cnt, long long* total,
+                               int* idx, cudaStream_t s);
+cudaError_t adr_launch_chunk_means(const AdrDev& d, AdrCtrl* ctrl, const float** src_slot,
+                                   float* means_out, cudaStream_t s);
+cudaError_t adr_launch_flags(const uint8_t* mat, const Grid& g, int nd, int pore, int bfc,
+                             uint32_t* flags, uint8_t* mflag, cudaStream_t s);
+cudaError_t adr_launch_vel_stats(const float* vel, const AdrDev& d, float* tmp, float* means,
+                                 unsigned* vmax_bits, unsigned long long* nbf, cudaStream_t s);
+}  // namespace prt
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t want) {
+        if (want <= bytes && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, want ? want : 1);
+        if (e == cudaSuccess) bytes = want;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+struct GraphHolder {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool conditional = false;
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+};
+
+struct FlowKey {
+    int nd = 0, precision = -1, every = 0;
+    Grid g{0, 0, 0, 0};
+    double force = 0, tau = 0, magic = 0;
+    long long nit = -1;
+    double tol = 0;
+    void* f = nullptr;
+    void* aux[3] = {nullptr, nullptr, nullptr};
+    bool operator==(const FlowKey& o) const {
+        return nd == o.nd && precision == o.precision && every == o.every && g.nx == o.g.nx &&
+               g.ny == o.g.ny && g.nz == o.g.nz && force == o.force && tau == o.tau &&
+               magic == o.magic && nit == o.nit && tol == o.tol && f == o.f && aux[0] == o.aux[0] &&
+               aux[1] == o.aux[1] && aux[2] == o.aux[2];
+    }
+};
+
+struct FlowState {
+    DevBuf f, fluid, partials, ctrl, out5, count, mat, vel;
+    GraphHolder graph;
+    FlowKey key;
+};
+
+struct AdrState {
+    bool begun = false;
+    bool ran = false;
+    prt_adr_params p{};
+    AdrDev d{};
+    DevBuf mat, vel, flags, mflag, face[3], buf[2], ladder, slot_of_step, idx, cnt, total;
+    DevBuf tree_leaf_start, tree_leaf_len, tree_inner_l, tree_inner_r, tree_level_off, tree_vals;
+    DevBuf means, src_slot, ctrl, log;
+    bool staged = false;
+    prt_adr_geom geom{};
+    const uint8_t* d_mat = nullptr;  // staged inputs (borrowed until begin)
+    const float* d_vel = nullptr;
+    DevBuf tmp, vstats;
+    std::vector<long long> keep_steps;  // ladder step numbers
+    std::vector<int> slot_of_index;     // ladder index -> slot
+    int nslots = 0;
+    GraphHolder graph;
+    void release() {
+        DevBuf* all[] = {&mat, &vel, &flags, &mflag, &face[0], &face[1], &face[2], &buf[0], &buf[1],
+                         &ladder, &slot_of_step, &idx, &cnt, &total, &tree_leaf_start,
+                         &tree_leaf_len, &tree_inner_l, &tree_inner_r, &tree_level_off, &tree_vals,
+                         &means, &src_slot, &ctrl, &log, &tmp, &vstats};
+        for (DevBuf* b : all) b->release();
+        staged = false;
+        graph.release();
+        keep_steps.clear();
+        slot_of_index.clear();
+        begun = ran = false;
+    }
+};
+
+}  // namespace
+
+struct prt_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    double timing[4] = {0, 0, 0, 0};
+    FlowState flow;
+    AdrState adr;
+};
+
+namespace {
+
+int fail(prt_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(prt_ctx* c, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return fail(c, e == cudaErrorMemoryAllocation ? PRT_E_OOM : PRT_E_CUDA, m);
+}
+
+#define CK(expr)                                                   \
+    do {                                                           \
+        cudaError_t _e = (expr);                                   \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, #expr);   \
+    } while (0)
+
+bool graphs_disabled() {
+    const char* v = std::getenv("PRT_GRAPHS");
+    return v && v[0] == '0';
+}
+
+// Build "while (cond) { body }" as a graph; body is captured from `emit`.
+// Falls back to a plain graph of the body when conditional nodes are
+// unavailable (the host then relaunches it until the control block says done).
+template <class Emit>
+cudaError_t build_while_graph(cudaStream_t s, GraphHolder& gh, Emit emit) {
+    gh.release();
+    cudaError_t e = cudaGraphCreate(&gh.graph, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle handle;
+    e = cudaGraphConditionalHandleCreate(&handle, gh.graph, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        e = cudaGraphAddNode(&node, gh.graph, nullptr, 0, &cp);
+        if (e == cudaSuccess) {
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                cudaError_t ee = emit(handle, 1);
+                cudaGraph_t outg = nullptr;
+                e = cudaStreamEndCapture(s, &outg);
+                if (ee != cudaSuccess) e = ee;
+                if (e == cudaSuccess) {
+                    e = cudaGraphInstantiate(&gh.exec, gh.graph, 0);
+                    if (e == cudaSuccess) {
+                        gh.conditional = true;
+                        return cudaSuccess;
+                    }
+                }
+            }
+        }
+    }
+    // fallback: plain body graph
+    cudaGetLastError();
+    gh.release();
+    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    cudaError_t ee = emit(cudaGraphConditionalHandle(0), 0);
+    e = cudaStreamEndCapture(s, &gh.graph);
+    if (ee != cudaSuccess) return ee;
+    if (e != cudaSuccess) return e;
+    e = cudaGraphInstantiate(&gh.exec, gh.graph, 0);
+    gh.conditional = false;
+    return e;
+}
+
+__global__ void count_fluid_kernel(const uint8_t* __restrict__ fluid, long long n,
+                                   unsigned long long* out) {
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int v = (c < n && fluid[c]) ? 1 : 0;
+    v = __syncthreads_count(v);
+    if (threadIdx.x == 0 && v) atomicAdd(out, (unsigned long long)v);
+}
+
+Grid make_grid(int nd, const int32_t* dims) {
+    Grid g;
+    if (nd == 3) {
+        g.nx = dims[0];
+        g.ny = dims[1];
+        g.nz = dims[2];
+    } else {
+        g.nx = dims[0];
+        g.ny = 1;
+        g.nz = dims[1];
+    }
+    g.n = (long long)g.nx * g.ny * g.nz;
+    return g;
+}
+
+template <class R>
+void fill_lbconst(LbConst<R>& k, int nd, double force, double tau, double magic, float scale) {
+    // _trt_minus (prtlb_3d.py:130-139)
+    const double om_p = 1.0 / tau;
+    const double lam_p = 1.0 / om_p - 0.5;
+    const double om_m = 1.0 / (magic / lam_p + 0.5);
+    k.omp = (R)om_p;
+    k.omm = (R)om_m;
+    k.half_g = (R)(0.5 * force);
+    for (int p = 0; p < 9; ++p) k.guo[p] = (R)0;
+    // first member of each pair and its x component
+    if (nd == 3) {
+        // pairs (1,2) (3,4) ... (17,18); e_x of 1,7,9,11,13 is +1, of 3,5,15,17 is 0
+        const int pa[9] = {1, 3, 5, 7, 9, 11, 13, 15, 17};
+        const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+        for (int p = 0; p < 9; ++p) {
+            const int a = pa[p];
+            const double w = a < 7 ? 1.0 / 18.0 : 1.0 / 36.0;
+            k.guo[p] = (R)(w * (1 - 0.5 * om_m) * 3.0 * force * ex[a]);
+        }
+    } else {
+        const int pa[4] = {1, 2, 5, 6};
+        const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+        for (int p = 0; p < 4; ++p) {
+            const int a = pa[p];
+            const double w = a < 5 ? 1.0 / 9.0 : 1.0 / 36.0;
+            k.guo[p] = (R)(w * (1 - 0.5 * om_m) * 3.0 * force * ex[a]);
+        }
+    }
+    k.scale = scale;
+    k.inv_scale = 1.0f / scale;
+}
+
+}  // namespace
+
+// ===========================================================================
+// context
+// ===========================================================================
+extern "C" int prt_abi_version(void) { return PRT_ABI_VERSION; }
+
+extern "C" int prt_create(int device, prt_ctx** out) {
+    if (!out) return PRT_E_INVALID;
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        g_create_error = std::string("no CUDA device: ") + cudaGetErrorString(e);
+        cudaGetLastError();
+        return PRT_E_NODEV;
+    }
+    if (device < 0 || device >= n) {
+        g_create_error = "device index out of range";
+        return PRT_E_INVALID;
+    }
+    prt_ctx* c = new (std::nothrow) prt_ctx();
+    if (!c) return PRT_E_OOM;
+    c->device = device;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("cuda init failed: ") + cudaGetErrorString(e);
+        delete c;
+        return PRT_E_CUDA;
+    }
+    *out = c;
+    return PRT_OK;
+}
+
+extern "C" void prt_destroy(prt_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    c->adr.release();
+    FlowState& f = c->flow;
+    DevBuf* all[] = {&f.f, &f.fluid, &f.partials, &f.ctrl, &f.out5, &f.count, &f.mat, &f.vel};
+    for (DevBuf* b : all) b->release();
+    f.graph.release();
+    for (int i = 0; i < 4; ++i)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" const char* prt_last_error(const prt_ctx* c) {
+    return c ? c->err.c_str() : g_create_error.c_str();
+}
+
+extern "C" int64_t prt_kernel_launches(const prt_ctx* c) { return c ? c->launches : 0; }
+
+extern "C" void* prt_stream(const prt_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" int prt_last_timing(const prt_ctx* c, double* out4) {
+    if (!c || !out4) return PRT_E_INVALID;
+    for (int i = 0; i < 4; ++i) out4[i] = c->timing[i];
+    return PRT_OK;
+}
+
+extern "C" size_t prt_sizeof(int which) {
+    switch (which) {
+        case 0: return sizeof(prt_flow_params);
+        case 1: return sizeof(prt_flow_info);
+        case 2: return sizeof(prt_adr_params);
+        case 3: return sizeof(prt_adr_run_params);
+        case 4: return sizeof(prt_adr_result);
+        case 5: return sizeof(prt_adr_geom);
+        case 6: return sizeof(prt_adr_stats);
+        default: return 0;
+    }
+}
+
+// ===========================================================================
+// flow
+// ===========================================================================
+extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p,
+                            float* d_vel, prt_flow_info* info) {
+    if (!ctx || !p || !d_mat || !d_vel) return fail(ctx, PRT_E_INVALID, "null argument");
+    if (p->nd != 2 && p->nd != 3) return fail(ctx, PRT_E_INVALID, "nd must be 2 or 3");
+    for (int i = 0; i < p->nd; ++i)
+        if (p->dims[i] <= 0) return fail(ctx, PRT_E_INVALID, "grid dimensions must be positive");
+    if (!(p->tau > 0.5))
+        return fail(ctx, PRT_E_INVALID,
+                    "tau must exceed 0.5; the viscosity (tau-1/2)/3 is negative below it and the "
+                    "solver cannot run.");
+    if (p->every <= 0 || (p->every & 1))
+        return fail(ctx, PRT_E_INVALID, "the convergence interval must be a positive even number");
+    if (p->precision < PRT_FP64 || p->precision > PRT_FP16)
+        return fail(ctx, PRT_E_INVALID, "unknown precision");
+    if (p->nit < 0) return fail(ctx, PRT_E_INVALID, "negative iteration cap");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    FlowState& F = ctx->flow;
+    const Grid g = make_grid(p->nd, p->dims);
+    const int Q = p->nd == 3 ? 19 : 9;
+    const size_t es = p->precision == PRT_FP64 ? 8 : (p->precision == PRT_FP32 ? 4 : 2);
+    const int nb = flow_blocks(g);
+    CK(F.f.ensure((size_t)Q * g.n * es));
+    CK(F.fluid.ensure((size_t)g.n));
+    CK(F.partials.ensure((size_t)nb * 5 * sizeof(double)));
+    CK(F.ctrl.ensure(sizeof(FlowCtrl)));
+    CK(F.out5.ensure(8 * sizeof(double)));
+    CK(F.count.ensure(sizeof(unsigned long long)));
+
+    // pore mask and its size
+    CK(flow_launch_fluid_mask(d_mat, F.fluid.as<uint8_t>(), g.n, 2, s));
+    CK(cudaMemsetAsync(F.count.p, 0, sizeof(unsigned long long), s));
+    count_fluid_kernel<<<(unsigned)((g.n + 255) / 256), 256, 0, s>>>(
+        F.fluid.as<uint8_t>(), g.n, F.count.as<unsigned long long>());
+    CK(cudaGetLastError());
+    ctx->launches += 2;
+    unsigned long long nfluid = 0;
+    CK(cudaMemcpyAsync(&nfluid, F.count.p, sizeof(nfluid), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+
+    // f = w_i everywhere: shifted storage h = 0
+    CK(cudaMemsetAsync(F.f.p, 0, (size_t)Q * g.n * es, s));
+    FlowCtrl hc{};
+    hc.it_base = 0;
+    hc.nit = p->nit;
+    hc.iters = 0;
+    hc.nfluid = (long long)nfluid;
+    hc.tol = p->tol;
+    hc.prev = 0;
+    hc.change = INFINITY;
+    hc.every = p->every;
+    hc.done = p->nit == 0 ? 1 : 0;
+    CK(cudaMemcpyAsync(F.ctrl.p, &hc, sizeof(hc), cudaMemcpyHostToDevice, s));
+
+    float scale = 1.f;
+    if (p->precision == PRT_FP16) {
+        const double g0 = std::fabs(p->force) > 0 ? std::fabs(p->force) : 1e-6;
+        scale = (float)std::ldexp(1.0, (int)std::floor(std::log2(1.0 / g0)));
+    }
+    LbConst<double> kd;
+    LbConst<float> kf;
+    fill_lbconst(kd, p->nd, p->force, p->tau, p->magic, scale);
+    fill_lbconst(kf, p->nd, p->force, p->tau, p->magic, scale);
+    // float64 and float32 storage collide in float64; float16 storage in float32
+    const void* kc = p->precision == PRT_FP16 ? (const void*)&kf : (const void*)&kd;
+
+    FlowCtrl* dctrl = F.ctrl.as<FlowCtrl>();
+    double* parts = F.partials.as<double>();
+    const int every = p->every;
+    auto emit = [&](cudaGraphConditionalHandle h, int use) -> cudaError_t {
+        for (int k = 0; k < every; ++k) {
+            cudaError_t e = flow_launch_step(p->nd, p->precision, (k & 1) != 0, k == every - 1,
+                                             F.f.p, F.fluid.as<uint8_t>(), g, kc, dctrl, k, parts, s);
+            if (e != cudaSuccess) return e;
+        }
+        return flow_launch_check(dctrl, parts, nb, h, use, s);
+    };
+    CK(cudaEventRecord(ctx->ev[0], s));
+    if (hc.done == 0) {
+        if (graphs_disabled()) {
+            // direct launches, chunk by chunk
+            FlowCtrl hc2 = hc;
+            while (!hc2.done) {
+                CK(emit(cudaGraphConditionalHandle(0), 0));
+                ctx->launches += every + 1;
+                CK(cudaMemcpyAsync(&hc2, dctrl, sizeof(hc2), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+            }
+        } else {
+            FlowKey key;
+            key.nd = p->nd; key.precision = p->precision; key.every = every; key.g = g;
+            key.force = p->force; key.tau = p->tau; key.magic = p->magic; key.nit = p->nit;
+            key.tol = p->tol; key.f = F.f.p;
+            key.aux[0] = F.fluid.p; key.aux[1] = F.partials.p; key.aux[2] = F.ctrl.p;
+            if (!F.graph.exec || !(key == F.key)) {
+                CK(build_while_graph(s, F.graph, emit));
+                F.key = key;
+            }
+            const long long chunks = (p->nit + every - 1) / every;
+            if (F.graph.conditional) {
+                CK(cudaGraphLaunch(F.graph.exec, s));
+                FlowCtrl hc2;
+                CK(cudaMemcpyAsync(&hc2, dctrl, sizeof(hc2), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+                ctx->launches += (hc2.iters + every - 1) / every * (every + 1);
+            } else {
+                FlowCtrl hc2 = hc;
+                long long launched = 0;
+                while (!hc2.done && launched < chunks) {
+                    for (int r = 0; r < 20 && launched < chunks; ++r, ++launched)
+                        CK(cudaGraphLaunch(F.graph.exec, s));
+                    CK(cudaMemcpyAsync(&hc2, dctrl, sizeof(hc2), cudaMemcpyDeviceToHost, s));
+                    CK(cudaStreamSynchronize(s));
+                }
+                ctx->launches += launched * (every + 1);
+            }
+        }
+    }
+    CK(cudaEventRecord(ctx->ev[1], s));
+    FlowCtrl res;
+    CK(cudaMemcpyAsync(&res, dctrl, sizeof(res), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+        ctx->timing[0] = ms;
+        ctx->timing[1] = (double)res.iters;
+    }
+    // final field from the state after `iters` iterations
+    CK(flow_launch_moments(p->nd, p->precision, (res.iters & 1) != 0, F.f.p, F.fluid.as<uint8_t>(),
+                           g, kc, d_vel, parts, s));
+    CK(flow_launch_final_reduce(parts, nb, F.out5.as<double>(), s));
+    ctx->launches += 2;
+    double o5[5];
+    CK(cudaMemcpyAsync(o5, F.out5.p, sizeof(o5), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (info) {
+        memset(info, 0, sizeof(*info));
+        info->iters = res.iters;
+        info->converged = res.converged;
+        info->change = res.change;
+        info->fluid_cells = (int64_t)nfluid;
+        info->ux_sum = o5[0];
+        info->mass = o5[1];
+        info->speed_sum = o5[2];
+        info->umax = o5[3];
+        info->nonfinite = (int64_t)llround(o5[4]);
+        const double nu = (p->tau - 0.5) / 3.0;
+        info->permeability = p->force != 0 ? nu * (o5[0] / (double)g.n) / p->force : 0.0;
+        info->fp16_scale = scale;
+    }
+    return PRT_OK;
+}
+
+extern "C" int prt_flow(prt_ctx* ctx, const uint8_t* mat, const prt_flow_params* p, float* vel_out,
+                        prt_flow_info* info) {
+    if (!ctx || !p || !mat || !vel_out) return fail(ctx, PRT_E_INVALID, "null argument");
+    if (p->nd != 2 && p->nd != 3) return fail(ctx, PRT_E_INVALID, "nd must be 2 or 3");
+    for (int i = 0; i < p->nd; ++i)
+        if (p->dims[i] <= 0) return fail(ctx, PRT_E_INVALID, "grid dimensions must be positive");
+    CK(cudaSetDevice(ctx->device));
+    const Grid g = make_grid(p->nd, p->dims);
+    FlowState& F = ctx->flow;
+    CK(F.mat.ensure((size_t)g.n));
+    CK(F.vel.ensure((size_t)g.n * 3 * sizeof(float)));
+    CK(cudaMemcpyAsync(F.mat.p, mat, (size_t)g.n, cudaMemcpyHostToDevice, ctx->stream));
+    int rc = prt_flow_dev(ctx, F.mat.as<uint8_t>(), p, F.vel.as<float>(), info);
+    if (rc != PRT_OK) return rc;
+    CK(cudaMemcpyAsync(vel_out, F.vel.p, (size_t)g.n * 3 * sizeof(float), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+// ===========================================================================
+// transport
+// ===========================================================================
+namespace {
+
+struct TreeBuild {
+    std::vector<int> leaf_start, leaf_len;
+    std::vector<int> in_l, in_r, in_h;  // children encoded: >= 0 leaf id, < 0 -(inner id) - 1
+    std::vector<int> leaf_h;
+    int build(long long start, long long n) {
+        if (n <= 128) {
+            leaf_start.push_back((int)start);
+            leaf_len.push_back((int)n);
+            return (int)leaf_start.size() - 1;
+        }
+        long long n2 = n / 2;
+        n2 -= n2 % 8;
+        int l = build(start, n2);
+        int r = build(start + n2, n - n2);
+        in_l.push_back(l);
+        in_r.push_back(r);
+        const int hl = l >= 0 ? 0 : in_h[-l - 1];
+        const int hr = r >= 0 ? 0 : in_h[-r - 1];
+        in_h.push_back(std::max(hl, hr) + 1);
+        return -(int)in_l.size();
+    }
+};
+
+}  // namespace
+
+extern "C" int prt_adr_stage_dev(prt_ctx* ctx, const uint8_t* d_mat, const float* d_vel,
+                                 const prt_adr_geom* geom, prt_adr_stats* stats) {
+    if (!ctx || !geom || !d_mat || !d_vel) return fail(ctx, PRT_E_INVALID, "null argument");
+    if (geom->nd != 2 && geom->nd != 3) return fail(ctx, PRT_E_INVALID, "grid must be 2D or 3D");
+    for (int i = 0; i < geom->nd; ++i)
+        if (geom->dims[i] <= 0) return fail(ctx, PRT_E_INVALID, "grid dimensions must be positive");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    AdrState& A = ctx->adr;
+    A.graph.release();
+    A.keep_steps.clear();
+    A.slot_of_index.clear();
+    A.begun = A.ran = false;
+    A.staged = false;
+    A.geom = *geom;
+    const Grid g = make_grid(geom->nd, geom->dims);
+    const long long N = g.n;
+    A.d.g = g;
+    A.d.nd = geom->nd;
+    CK(A.flags.ensure((size_t)N * 4));
+    CK(A.mflag.ensure((size_t)N));
+    A.d.flags = A.flags.as<uint32_t>();
+    CK(adr_launch_flags(d_mat, g, geom->nd, geom->pore_code, geom->biofilm_code,
+                        A.flags.as<uint32_t>(), A.mflag.as<uint8_t>(), s));
+    // compressed solute voxel list
+    const int nbs = (int)((N + 1023) / 1024);
+    CK(A.cnt.ensure((size_t)nbs * 4));
+    CK(A.total.ensure(8));
+    CK(adr_launch_compact(A.mflag.as<uint8_t>(), N, A.cnt.as<int>(), A.total.as<long long>(),
+                          nullptr, s));
+    long long nm = 0;
+    CK(cudaMemcpyAsync(&nm, A.total.p, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(A.idx.ensure((size_t)std::max(nm, 1ll) * 4));
+    CK(adr_launch_compact(A.mflag.as<uint8_t>(), N, A.cnt.as<int>(), A.total.as<long long>(),
+                          A.idx.as<int>(), s));
+    ctx->launches += 6;
+    A.d.idx = A.idx.as<int>();
+    A.d.nm = nm;
+    // numpy pairwise tree over nm values
+    TreeBuild tb;
+    int root = -1;
+    if (nm > 0) root = tb.build(0, nm);
+    const int L = (int)tb.leaf_start.size();
+    const int I = (int)tb.in_l.size();
+    // order inner nodes by height
+    std::vector<int> order(I);
+    for (int i = 0; i < I; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tb.in_h[a] < tb.in_h[b]; });
+    std::vector<int> rank(I);
+    for (int r = 0; r < I; ++r) rank[order[r]] = r;
+    auto enc = [&](int id) { return id >= 0 ? id : L + rank[-id - 1]; };
+    std::vector<int> il(std::max(I, 1)), ir(std::max(I, 1));
+    for (int r = 0; r < I; ++r) {
+        const int i = order[r];
+        il[r] = enc(tb.in_l[i]);
+        ir[r] = enc(tb.in_r[i]);
+    }
+    // inner nodes of height h+1 occupy [loff[h], loff[h+1])
+    const int nlevel = I > 0 ? tb.in_h[order[I - 1]] : 0;
+    std::vector<int> loff(nlevel + 1, 0);
+    for (int r = 0; r < I; ++r) loff[tb.in_h[order[r]]] += 1;
+    for (int h = 1; h <= nlevel; ++h) loff[h] += loff[h - 1];
+    CK(A.tree_leaf_start.ensure((size_t)std::max(L, 1) * 4));
+    CK(A.tree_leaf_len.ensure((size_t)std::max(L, 1) * 4));
+    CK(A.tree_inner_l.ensure((size_t)std::max(I, 1) * 4));
+    CK(A.tree_inner_r.ensure((size_t)std::max(I, 1) * 4));
+    CK(A.tree_level_off.ensure((size_t)(nlevel + 1) * 4));
+    CK(A.tree_vals.ensure((size_t)std::max(L + I, 1) * PRT_MAX_SPECIES * 4));
+    if (L) {
+        CK(cudaMemcpyAsync(A.tree_leaf_start.p, tb.leaf_start.data(), (size_t)L * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(A.tree_leaf_len.p, tb.leaf_len.data(), (size_t)L * 4, cudaMemcpyHostToDevice, s));
+    }
+    if (I) {
+        CK(cudaMemcpyAsync(A.tree_inner_l.p, il.data(), (size_t)I * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(A.tree_inner_r.p, ir.data(), (size_t)I * 4, cudaMemcpyHostToDevice, s));
+    }
+    CK(cudaMemcpyAsync(A.tree_level_off.p, loff.data(), (size_t)(nlevel + 1) * 4, cudaMemcpyHostToDevice, s));
+    A.d.tree.nleaf = L;
+    A.d.tree.ninner = I;
+    A.d.tree.nlevel = nlevel;
+    A.d.tree.root = nm > 0 ? enc(root) : -1;
+    A.d.tree.leaf_start = A.tree_leaf_start.as<int>();
+    A.d.tree.leaf_len = A.tree_leaf_len.as<int>();
+    A.d.tree.inner_l = A.tree_inner_l.as<int>();
+    A.d.tree.inner_r = A.tree_inner_r.as<int>();
+    A.d.tree.level_off = A.tree_level_off.as<int>();
+    A.d.tree_vals = A.tree_vals.as<float>();
+    CK(A.means.ensure(PRT_MAX_SPECIES * 4));
+    CK(A.src_slot.ensure(sizeof(float*)));
+    CK(A.ctrl.ensure(sizeof(AdrCtrl)));
+    // velocity statistics for the host's set-up
+    CK(A.tmp.ensure((size_t)N * 4));
+    CK(A.vstats.ensure(64));
+    CK(cudaMemsetAsync(A.vstats.p, 0, 64, s));
+    float* vs_means = A.vstats.as<float>();                                  // 2 floats
+    unsigned* vs_max = reinterpret_cast<unsigned*>(A.vstats.as<char>() + 16);  // 3 uints
+    unsigned long long* vs_bf = reinterpret_cast<unsigned long long*>(A.vstats.as<char>() + 32);
+    CK(adr_launch_vel_stats(d_vel, A.d, A.tmp.as<float>(), vs_means, vs_max, vs_bf, s));
+    ctx->launches += 8;
+    unsigned char hv[64];
+    CK(cudaMemcpyAsync(hv, A.vstats.p, 64, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));  // host vectors above go out of scope
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->solute_voxels = nm;
+        memcpy(&stats->biofilm_voxels, hv + 32, 8);
+        memcpy(&stats->mean_axial, hv, 4);
+        memcpy(&stats->mean_speed, hv + 4, 4);
+        memcpy(stats->vmax, hv + 16, 12);
+    }
+    A.d_mat = d_mat;
+    A.d_vel = d_vel;
+    A.staged = true;
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_stage(prt_ctx* ctx, const uint8_t* mat, const float* vel,
+                             const prt_adr_geom* geom, prt_adr_stats* stats) {
+    if (!ctx || !geom || !mat || !vel) return fail(ctx, PRT_E_INVALID, "null argument");
+    if (geom->nd != 2 && geom->nd != 3) return fail(ctx, PRT_E_INVALID, "grid must be 2D or 3D");
+    for (int i = 0; i < geom->nd; ++i)
+        if (geom->dims[i] <= 0) return fail(ctx, PRT_E_INVALID, "grid dimensions must be positive");
+    CK(cudaSetDevice(ctx->device));
+    const Grid g = make_grid(geom->nd, geom->dims);
+    AdrState& A = ctx->adr;
+    CK(A.mat.ensure((size_t)g.n));
+    CK(A.vel.ensure((size_t)g.n * 3 * 4));
+    CK(cudaMemcpyAsync(A.mat.p, mat, (size_t)g.n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(A.vel.p, vel, (size_t)g.n * 3 * 4, cudaMemcpyHostToDevice, ctx->stream));
+    return prt_adr_stage_dev(ctx, A.mat.as<uint8_t>(), A.vel.as<float>(), geom, stats);
+}
+
+extern "C" int prt_adr_begin(prt_ctx* ctx, const prt_adr_params* p) {
+    if (!ctx || !p) return fail(ctx, PRT_E_INVALID, "null argument");
+    AdrState& A = ctx->adr;
+    if (!A.staged) return fail(ctx, PRT_E_STATE, "prt_adr_begin before prt_adr_stage");
+    if (p->nd != A.geom.nd || p->pore_code != A.geom.pore_code ||
+        p->biofilm_code != A.geom.biofilm_code)
+        return fail(ctx, PRT_E_INVALID, "parameters do not match the staged geometry");
+    for (int i = 0; i < p->nd; ++i)
+        if (p->dims[i] != A.geom.dims[i])
+            return fail(ctx, PRT_E_INVALID, "parameters do not match the staged geometry");
+    if (p->ns < 1 || p->ns > PRT_MAX_SPECIES)
+        return fail(ctx, PRT_E_INVALID, "between 1 and 8 chemicals are supported");
+    if (!(p->dt > 0.f)) return fail(ctx, PRT_E_INVALID, "the time step must be positive");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    A.graph.release();
+    A.p = *p;
+    const Grid g = A.d.g;
+    const long long N = g.n;
+    A.d.ns = p->ns;
+    for (int a = 0; a < 3; ++a) {
+        const int ext = a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
+        const bool active = (p->nd == 3) || a != 1;
+        CK(A.face[a].ensure(active ? (size_t)(N / ext * (ext + 1)) * 4 : 4));
+        A.d.face[a] = A.face[a].as<float>();
+    }
+    CK(A.buf[0].ensure((size_t)N * p->ns * 4));
+    CK(A.buf[1].ensure((size_t)N * p->ns * 4));
+    CK(cudaMemsetAsync(A.buf[1].p, 0, (size_t)N * p->ns * 4, s));
+    A.d.buf[0] = A.buf[0].as<float>();
+    A.d.buf[1] = A.buf[1].as<float>();
+    A.d.ladder = nullptr;  // allocated by prt_adr_run
+    CK(adr_launch_setup(A.d_mat, A.d_vel, *p, A.d, s));
+    ctx->launches += p->nd + 1;
+    CK(cudaStreamSynchronize(s));
+    A.begun = true;
+    A.ran = false;
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progress_cb cb,
+                           void* user, prt_adr_result* res) {
+    if (!ctx || !rp) return fail(ctx, PRT_E_INVALID, "null argument");
+    AdrState& A = ctx->adr;
+    if (!A.begun) return fail(ctx, PRT_E_STATE, "prt_adr_run before prt_adr_begin");
+    if (rp->limit < 0 || rp->check <= 0 || !(rp->ratio > 0))
+        return fail(ctx, PRT_E_INVALID, "bad run parameters");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const long long N = A.d.g.n;
+    const int ns = A.p.ns;
+    const long long limit = rp->limit;
+    // the snapshot ladder (prtlb_3d.py:1496-1498): record at n >= nxt,
+    // nxt = max(n + 1, ceil(n * ratio)); steps are known before the run
+    std::vector<long long> sched;
+    {
+        long long nxt = 1;
+        for (long long n = nxt; n <= limit;) {
+            sched.push_back(n);
+            long long c2 = (long long)std::ceil((double)n * rp->ratio);
+            nxt = std::max(n + 1, c2);
+            n = nxt;
+        }
+    }
+    const int K = (int)sched.size();
+    A.nslots = K + 2;  // step 0, the schedule, and a final record
+    const size_t slot_bytes = (size_t)N * ns * 4;
+    CK(A.ladder.ensure(slot_bytes * A.nslots));
+    CK(cudaMemsetAsync(A.ladder.p, 0, slot_bytes * A.nslots, s));
+    CK(cudaMemcpyAsync(A.ladder.p, A.buf[0].p, slot_bytes, cudaMemcpyDeviceToDevice, s));
+    std::vector<int> sos((size_t)limit + 1, -1);
+    for (int k = 0; k < K; ++k) sos[(size_t)sched[k]] = k + 1;
+    CK(A.slot_of_step.ensure(sos.size() * 4));
+    CK(cudaMemcpyAsync(A.slot_of_step.p, sos.data(), sos.size() * 4, cudaMemcpyHostToDevice, s));
+    const int log_cap = (int)(limit / rp->check) + 2;
+    CK(A.log.ensure((size_t)log_cap * sizeof(ProgressRec)));
+    A.d.ladder = A.ladder.as<float>();
+    A.d.slot_of_step = A.slot_of_step.as<int>();
+    A.d.log = A.log.as<ProgressRec>();
+    A.d.log_cap = log_cap;
+
+    AdrCtrl hc{};
+    hc.n_base = 0;
+    hc.limit = limit;
+    hc.check = rp->check;
+    hc.until_conv = rp->until_conv;
+    hc.tol = rp->tol;
+    hc.ns = ns;
+    hc.last_rest = INFINITY;
+    for (int j = 0; j < PRT_MAX_SPECIES; ++j) {
+        hc.prev[j] = 0.0;
+        hc.prev_change[j] = 0.0;
+        hc.scale[j] = 1e-6;
+    }
+    // with a progress callback the host regains control every few checks
+    long long pause_every = cb ? (long long)rp->check * 8 : limit;
+    hc.n_pause = std::min(limit, pause_every);
+    hc.done = limit == 0 ? 1 : 0;
+    AdrCtrl* dctrl = A.ctrl.as<AdrCtrl>();
+    CK(cudaMemcpyAsync(dctrl, &hc, sizeof(hc), cudaMemcpyHostToDevice, s));
+
+    const int check = rp->check;
+    const prt_adr_params P = A.p;
+    const AdrDev D = A.d;
+    float* dmeans = A.means.as<float>();
+    const float** srcp = (const float**)A.src_slot.p;
+    auto emit = [&](cudaGraphConditionalHandle h, int use) -> cudaError_t {
+        for (int k = 0; k < check; ++k) {
+            cudaError_t e = adr_launch_step(D, P, dctrl, k, s);
+            if (e != cudaSuccess) return e;
+        }
+        cudaError_t e = adr_launch_chunk_means(D, dctrl, srcp, dmeans, s);
+        if (e != cudaSuccess) return e;
+        return adr_launch_stop(D, dctrl, dmeans, h, use, s);
+    };
+    const int per_chunk = check + 3 + (D.tree.nleaf > 0 ? 1 : 0);
+    std::vector<ProgressRec> logbuf;
+    int delivered = 0;
+    AdrCtrl cur = hc;
+    bool use_graph = !graphs_disabled();
+    if (use_graph && !cur.done) CK(build_while_graph(s, A.graph, emit));
+    CK(cudaEventRecord(ctx->ev[2], s));
+    while (!cur.done) {
+        if (!use_graph) {
+            CK(emit(cudaGraphConditionalHandle(0), 0));
+            ctx->launches += per_chunk;
+        } else if (A.graph.conditional) {
+            CK(cudaGraphLaunch(A.graph.exec, s));
+        } else {
+            for (int r = 0; r < 4; ++r) {
+                CK(cudaGraphLaunch(A.graph.exec, s));
+                ctx->launches += per_chunk;
+            }
+        }
+        const long long before = cur.n_base;
+        CK(cudaMemcpyAsync(&cur, dctrl, sizeof(cur), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (use_graph && A.graph.conditional)
+            ctx->launches += (cur.n_base - before + check - 1) / check * per_chunk;
+        if (cb && cur.nlog > delivered) {
+            const int nrec = std::min(cur.nlog, log_cap) - delivered;
+            logbuf.resize(nrec);
+            if (nrec > 0) {
+                CK(cudaMemcpy(logbuf.data(), A.d.log + delivered, nrec * sizeof(ProgressRec),
+                              cudaMemcpyDeviceToHost));
+            }
+            for (int i = 0; i < nrec; ++i) {
+                if (cb(user, logbuf[i].n, limit, logbuf[i].mean0, logbuf[i].value) != 0) {
+                    A.ran = true;
+                    return fail(ctx, PRT_E_CANCELLED, "cancelled by the progress callback");
+                }
+            }
+            delivered += nrec;
+        }
+        if (!cur.done && cur.n_base >= cur.n_pause) {
+            cur.n_pause = std::min(limit, cur.n_pause + pause_every);
+            CK(cudaMemcpyAsync(&dctrl->n_pause, &cur.n_pause, sizeof(long long),
+                               cudaMemcpyHostToDevice, s));
+        }
+    }
+    CK(cudaEventRecord(ctx->ev[3], s));
+    CK(cudaEventSynchronize(ctx->ev[3]));
+    {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+        ctx->timing[2] = ms;
+        ctx->timing[3] = (double)cur.n_base;
+    }
+    const long long n = cur.n_base;
+    // keep_steps = [0] + ladder steps <= n, plus n itself when not one of them
+    A.keep_steps.clear();
+    A.slot_of_index.clear();
+    A.keep_steps.push_back(0);
+    A.slot_of_index.push_back(0);
+    for (int k = 0; k < K && sched[k] <= n; ++k) {
+        A.keep_steps.push_back(sched[k]);
+        A.slot_of_index.push_back(k + 1);
+    }
+    if (A.keep_steps.back() != n) {
+        CK(cudaMemcpyAsync(A.ladder.as<char>() + slot_bytes * (K + 1), A.buf[n & 1].p, slot_bytes,
+                           cudaMemcpyDeviceToDevice, s));
+        A.keep_steps.push_back(n);
+        A.slot_of_index.push_back(K + 1);
+    }
+    CK(cudaStreamSynchronize(s));
+    A.ran = true;
+    if (res) {
+        memset(res, 0, sizeof(*res));
+        res->steps = n;
+        res->hit_cap = (rp->until_conv && n >= limit) ? 1 : 0;
+        res->ladder = (int32_t)A.keep_steps.size();
+        res->checks = cur.checks;
+        res->last_rest = cur.last_rest;
+    }
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_ladder(prt_ctx* ctx, int64_t* steps, int32_t cap, int32_t* count) {
+    if (!ctx) return PRT_E_INVALID;
+    AdrState& A = ctx->adr;
+    if (!A.ran) return fail(ctx, PRT_E_STATE, "no finished run");
+    const int n = (int)A.keep_steps.size();
+    if (count) *count = n;
+    if (steps)
+        for (int i = 0; i < n && i < cap; ++i) steps[i] = A.keep_steps[i];
+    return PRT_OK;
+}
+
+static int slot_ptr(prt_ctx* ctx, int32_t slot, const float** out) {
+    AdrState& A = ctx->adr;
+    if (!A.ran) return fail(ctx, PRT_E_STATE, "no finished run");
+    if (slot < 0 || slot >= (int)A.slot_of_index.size())
+        return fail(ctx, PRT_E_INVALID, "snapshot index out of range");
+    *out = A.ladder.as<float>() + (size_t)A.slot_of_index[slot] * A.d.g.n * A.p.ns;
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_fetch(prt_ctx* ctx, int32_t slot, float* out) {
+    if (!ctx || !out) return fail(ctx, PRT_E_INVALID, "null argument");
+    const float* src = nullptr;
+    int rc = slot_ptr(ctx, slot, &src);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    const size_t bytes = (size_t)ctx->adr.d.g.n * ctx->adr.p.ns * 4;
+    CK(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_fetch_dev(prt_ctx* ctx, int32_t slot, float* d_out) {
+    if (!ctx || !d_out) return fail(ctx, PRT_E_INVALID, "null argument");
+    const float* src = nullptr;
+    int rc = slot_ptr(ctx, slot, &src);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    const size_t bytes = (size_t)ctx->adr.d.g.n * ctx->adr.p.ns * 4;
+    CK(cudaMemcpyAsync(d_out, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_means(prt_ctx* ctx, int32_t slot, float* means) {
+    if (!ctx || !means) return fail(ctx, PRT_E_INVALID, "null argument");
+    AdrState& A = ctx->adr;
+    if (!A.ran) return fail(ctx, PRT_E_STATE, "no finished run");
+    if (slot < 0 || slot >= (int)A.slot_of_index.size())
+        return fail(ctx, PRT_E_INVALID, "snapshot index out of range");
+    CK(cudaSetDevice(ctx->device));
+    CK(adr_launch_means(A.d, A.ctrl.as<AdrCtrl>(), A.slot_of_index[slot], A.means.as<float>(),
+                        ctx->stream));
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(means, A.means.p, (size_t)A.p.ns * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_end(prt_ctx* ctx) {
+    if (!ctx) return PRT_E_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->adr.release();
+    return PRT_OK;
+}

@@ -1,0 +1,9 @@
+"""Drop-in for the reference module 3D/tools/prtlb_3d.py: the names its
+callers import (build_dataset_3d.py:70, build_practice_dataset.py:23-25)."""
+
+from . import SOLID, WALL, PORE  # noqa: F401
+from .adr import solve_adr, _wanted_steps, _nearest_unused  # noqa: F401
+from .chemistry import Chemistry, default_chemistry  # noqa: F401
+from .flow import stokes_d3q19, trt_minus as _trt_minus  # noqa: F401
+from .geometry import assert_finite_distance, coat_with_biofilm, keep_inlet_connected  # noqa: F401
+from .physics import check_physics  # noqa: F401

@@ -1,0 +1,89 @@
+"""Transport parity on the GPU: solve_adr through libprtlb.so against the
+reference's golden runs.  The bar is bit-identity: the reference integrates
+in float32 with numpy and the CUDA step replays its operation order with no
+fused multiply-add, and the stop rule's float32 means replay numpy's
+pairwise summation, so steps, snapshots, t_norm and the on_progress records
+must all be equal."""
+
+import contextlib
+import glob
+import io
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_golden
+from test_oracle_golden import adr_kwargs
+
+pytestmark = pytest.mark.gpu
+
+ADR32 = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "adr_*.npz")))
+
+
+def run(z, name, **extra):
+    from prtlb_gpu import solve_adr
+    kw = adr_kwargs(z, name)
+    kw.update(extra)
+    info = {}
+    prog = []
+    with contextlib.redirect_stdout(io.StringIO()):
+        out, tn = solve_adr(z["mat"], z["vel"], info=info,
+                            on_progress=lambda *a: prog.append(a), **kw)
+    return out, tn, info, np.asarray(prog, np.float64).reshape(-1, 4)
+
+
+@pytest.mark.parametrize("name", ADR32)
+def test_bit_identical_to_reference(name):
+    z = load_golden(name)
+    out, tn, info, prog = run(z, name)
+    assert info["steps"] == int(z["info_steps"])
+    assert info["ladder"] == int(z["info_ladder"])
+    assert info["dt"] == float(z["info_dt"])
+    assert info["converged"] == bool(z["info_converged"])
+    assert info["repeated_snapshots"] == int(z["info_repeated_snapshots"])
+    assert np.array_equal(tn, z["t_norm"])
+    assert np.array_equal(prog, z["progress"])
+    assert out.shape == z["out"].shape
+    assert np.array_equal(out, z["out"]), float(np.abs(out - z["out"]).max())
+
+
+def test_plug_flow_is_exp_minus_da():
+    from prtlb_gpu import solve_adr
+    for da in (0.5, 1.0, 2.0):
+        g = np.full((80, 8), 2, np.uint8)
+        v = np.zeros((3, 80, 8), np.float32)
+        v[0] = 1.0
+        with contextlib.redirect_stdout(io.StringIO()):
+            out, _ = solve_adr(g, v, pe=4000.0, da=da, n_t=3, n_species=1)
+        got = float(out[-1, 0, -1].mean())
+        assert abs(got - np.exp(-da)) < 0.05, (da, got)
+        assert out[-1].max() <= 1.0 + 1e-4
+    g3 = np.full((40, 6, 6), 2, np.uint8)
+    v3 = np.zeros((3, 40, 6, 6), np.float32)
+    v3[0] = 1.0
+    with contextlib.redirect_stdout(io.StringIO()):
+        out3, _ = solve_adr(g3, v3, pe=4000.0, da=1.0, n_t=3, n_species=1)
+    assert abs(float(out3[-1, 0, -1].mean()) - np.exp(-1.0)) < 0.06
+    assert out3.max() <= 1.0 + 1e-4
+
+
+def test_progress_callback_exception_propagates():
+    from prtlb_gpu import solve_adr
+    g = np.full((40, 8), 2, np.uint8)
+    v = np.zeros((3, 40, 8), np.float32)
+    v[0] = 1.0
+
+    class Stop(Exception):
+        pass
+
+    def cb(*a):
+        raise Stop()
+
+    with pytest.raises(Stop):
+        with contextlib.redirect_stdout(io.StringIO()):
+            solve_adr(g, v, pe=30.0, da=1.0, n_t=3, n_species=1, on_progress=cb)
+    # the context is usable afterwards
+    with contextlib.redirect_stdout(io.StringIO()):
+        out, _ = solve_adr(g, v, pe=30.0, da=1.0, n_t=3, n_species=1, steps=50)
+    assert np.isfinite(out).all()
