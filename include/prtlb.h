@@ -45,9 +45,11 @@ extern "C" {
 #define PRT_E_NODEV (-6)     /* no CUDA device */
 
 /* population storage for the flow solve */
-#define PRT_FP64 0 /* float64, as the reference                            */
-#define PRT_FP32 1 /* float32 holding f_i - w_i, collided in float64        */
-#define PRT_FP16 2 /* float16 holding (f_i - w_i) * 2^k, collided in float32 */
+#define PRT_FP64 0     /* float64, as the reference                             */
+#define PRT_FP32 1     /* float32 holding f_i - w_i; momentum and antisymmetric
+                          non-equilibrium part in float64, the rest in float32  */
+#define PRT_FP16 2     /* float16 holding (f_i - w_i) * 2^k, collided in float32 */
+#define PRT_FP32_F32 3 /* float32 holding f_i - w_i, collided in float32        */
 
 typedef struct prt_ctx prt_ctx;
 

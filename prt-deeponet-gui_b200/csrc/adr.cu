@@ -113,8 +113,12 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
         const float uL = face[a][fi];
         const float uH = face[a][fi + face_step(g, a)];
         const int bf = (fl & F_BF) ? 1 : 0;
-        const float DL = oL ? dj[bf + ((fl & f_nbf_lo(a)) ? 1 : 0)] : 0.f;
-        const float DH = oH ? dj[bf + ((fl & f_nbf_hi(a)) ? 1 : 0)] : 0.f;
+        // face diffusivity by the biofilm count of its two voxels (0, 1, 2);
+        // selected, not indexed, so the table stays in registers
+        const int nl = bf + ((fl & f_nbf_lo(a)) ? 1 : 0);
+        const int nh = bf + ((fl & f_nbf_hi(a)) ? 1 : 0);
+        const float DL = oL ? (nl == 0 ? dj[0] : (nl == 1 ? dj[1] : dj[2])) : 0.f;
+        const float DH = oH ? (nh == 0 ? dj[0] : (nh == 1 ? dj[1] : dj[2])) : 0.f;
         // out += D_hi (C+1 - C) + D_lo (C-1 - C)
         out = out + (DH * (Cp1 - Cc) + DL * (Cm1 - Cc));
         const float fh = (uH >= 0.f) ? muscl(Cc, Cm1, Cp1) : muscl(Cp1, Cp2, Cc);

@@ -1,0 +1,541 @@
+// lb_flow.cu -- lattice-Boltzmann Stokes flow kernels (D2Q9 / D3Q19, TRT, Guo
+// forcing, node bounce-back, periodic streaming) for sm_100a.
+//
+// What the reference does per iteration (prtlb_3d.py:427-445, prtlb_2d.py:449-474):
+//   moments rho, u (u_x gets +g/2, u = 0 on solid)  -> feq
+//   TRT collision (_trt_collide, prtlb_3d.py:142) + Guo term w_i(1-om-/2) 3 g e_ix
+//   solid voxels: post-collision = the reversed ARRIVED populations
+//   periodic streaming of every population (np.roll on every axis)
+//
+// Here one launch does one whole iteration as a pull from lattice Lr (the
+// post-collision populations of the previous iteration) into lattice Lw:
+// a pore voxel x gathers f_i from x - e_i, collides and writes its values
+// contiguously into its own slots of Lw.  When x - e_i is rock, the reference
+// rule "the solid voxel sends back what arrived there one iteration earlier"
+// makes the arriving value x's own post-collision population in direction
+// opp(i) from two iterations ago -- which is still in Lw[opp(i)][x], not yet
+// overwritten, and read by the same thread before it writes.  Solid voxels
+// therefore do no work at all, and the transient is the reference's, not
+// only its steady state.
+//
+// Populations are stored shifted, h_i = f_i - w_i: the non-equilibrium part
+// that carries the viscous stress is of the order of the force (1e-7) and
+// would drown next to w_i ~ 0.3 in float32 (prtlb_2d.py:354-362).
+#include <cuda_fp16.h>
+
+#include "prt_internal.h"
+
+namespace prt {
+
+// -------------------------------------------------------------------------
+// Lattices, in the storage frame (x, y, z).  The direction order and weights
+// are the reference's (prtlb_3d.py:370-375, prtlb_2d.py:391-394); a D2Q9
+// direction (ex, ey) is stored as (ex, 0, ey) because 2D grids are kept as
+// (nx, 1, ny).
+// -------------------------------------------------------------------------
+struct D3Q19 {
+    static constexpr int Q = 19;
+    static constexpr int NP = 9;
+    __host__ __device__ static constexpr int c(int i, int a) {
+        return (a == 0) ? (i == 1 || i == 7 || i == 9 || i == 11 || i == 13   ? 1
+                           : i == 2 || i == 8 || i == 10 || i == 12 || i == 14 ? -1
+                                                                                : 0)
+             : (a == 1) ? (i == 3 || i == 7 || i == 10 || i == 15 || i == 17   ? 1
+                           : i == 4 || i == 8 || i == 9 || i == 16 || i == 18  ? -1
+                                                                                : 0)
+                        : (i == 5 || i == 11 || i == 14 || i == 15 || i == 18  ? 1
+                           : i == 6 || i == 12 || i == 13 || i == 16 || i == 17 ? -1
+                                                                                 : 0);
+    }
+    // pairs (a, b) with e_b = -e_a
+    __host__ __device__ static constexpr int pa(int p) { return 2 * p + 1; }
+    __host__ __device__ static constexpr int pb(int p) { return 2 * p + 2; }
+    __host__ __device__ static constexpr int opp(int i) {
+        return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1);
+    }
+    __host__ __device__ static constexpr double w(int i) {
+        return i == 0 ? 1.0 / 3.0 : (i < 7 ? 1.0 / 18.0 : 1.0 / 36.0);
+    }
+};
+
+struct D2Q9 {
+    static constexpr int Q = 9;
+    static constexpr int NP = 4;
+    // reference order: (0,0) (1,0) (0,1) (-1,0) (0,-1) (1,1) (-1,1) (-1,-1) (1,-1)
+    __host__ __device__ static constexpr int ex(int i) {
+        return (i == 1 || i == 5 || i == 8) ? 1 : ((i == 3 || i == 6 || i == 7) ? -1 : 0);
+    }
+    __host__ __device__ static constexpr int ey(int i) {
+        return (i == 2 || i == 5 || i == 6) ? 1 : ((i == 4 || i == 7 || i == 8) ? -1 : 0);
+    }
+    __host__ __device__ static constexpr int c(int i, int a) {
+        return a == 0 ? ex(i) : (a == 1 ? 0 : ey(i));
+    }
+    __host__ __device__ static constexpr int pa(int p) { return p < 2 ? p + 1 : p + 3; }
+    __host__ __device__ static constexpr int pb(int p) { return p < 2 ? p + 3 : p + 5; }
+    __host__ __device__ static constexpr int opp(int i) {
+        return i == 0 ? 0 : (i < 5 ? ((i + 1) % 4) + 1 : ((i - 3) % 4) + 5);
+    }
+    __host__ __device__ static constexpr double w(int i) {
+        return i == 0 ? 4.0 / 9.0 : (i < 5 ? 1.0 / 9.0 : 1.0 / 36.0);
+    }
+};
+
+// storage conversions ------------------------------------------------------
+// Pop<S>::H is the register type a stored population is held in; st() rounds
+// the collision result to the storage type once.
+template <class S>
+struct Pop;
+template <>
+struct Pop<double> {
+    using H = double;
+    __device__ static double ld(const double* p, float) { return *p; }
+    template <class R>
+    __device__ static void st(double* p, R v, float) { *p = (double)v; }
+};
+template <>
+struct Pop<float> {
+    using H = float;
+    __device__ static float ld(const float* p, float) { return *p; }
+    template <class R>
+    __device__ static void st(float* p, R v, float) { *p = (float)v; }
+};
+template <>
+struct Pop<__half> {
+    using H = float;
+    __device__ static float ld(const __half* p, float inv) { return __half2float(*p) * inv; }
+    template <class R>
+    __device__ static void st(__half* p, R v, float scale) {
+        float s = (float)v * scale;
+        s = fminf(fmaxf(s, -65504.f), 65504.f);
+        *p = __float2half_rn(s);
+    }
+};
+
+// Precision modes: storage type S, arithmetic R for the symmetric part and
+// RA for the momentum and the antisymmetric non-equilibrium part (a small
+// difference of two O(u) numbers), and the resident 256-thread blocks per SM
+// the register budget is cut for.
+struct ModeF64 {  // the reference's arithmetic
+    using S = double;
+    using R = double;
+    using RA = double;
+    static constexpr int min_blocks = 2;
+};
+struct ModeF32 {  // float32 populations, float32 collision
+    using S = float;
+    using R = float;
+    using RA = float;
+    static constexpr int min_blocks = 3;
+};
+struct ModeF32D {  // float32 populations, float64 momentum
+    using S = float;
+    using R = float;
+    using RA = double;
+    static constexpr int min_blocks = 3;
+};
+struct ModeF16 {  // scaled float16 populations, float32 collision
+    using S = __half;
+    using R = float;
+    using RA = float;
+    static constexpr int min_blocks = 3;
+};
+
+// Gather the arrived populations of pore voxel c (see the file comment).
+// nb: bit i set when the upstream voxel c - e_i is rock.
+template <class L, class S>
+__device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __restrict__ lw, int c,
+                                       uint32_t nb, const Grid& g, long long N, float inv,
+                                       typename Pop<S>::H (&h)[L::Q]) {
+    const int z = c % g.nz;
+    const int t = c / g.nz;
+    const int y = t % g.ny;
+    const int x = t / g.ny;
+    const int syz = g.ny * g.nz;
+    h[0] = Pop<S>::ld(lr + c, inv);
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        if (nb & (1u << i)) {
+            h[i] = Pop<S>::ld(lw + (long long)L::opp(i) * N + c, inv);
+        } else {
+            const int dx = -L::c(i, 0), dy = -L::c(i, 1), dz = -L::c(i, 2);
+            int xx = x + dx, yy = y + dy, zz = z + dz;
+            if (dx) xx = xx < 0 ? g.nx - 1 : (xx >= g.nx ? 0 : xx);
+            if (dy) yy = yy < 0 ? g.ny - 1 : (yy >= g.ny ? 0 : yy);
+            if (dz) zz = zz < 0 ? g.nz - 1 : (zz >= g.nz ? 0 : zz);
+            h[i] = Pop<S>::ld(lr + (long long)i * N + (xx * syz + yy * g.nz + zz), inv);
+        }
+    }
+}
+
+template <class R, class RA>
+struct Moments {
+    R drho, jsq;    // density deviation, rho u^2
+    RA jx, jy, jz;  // J = rho u (with the half force on x)
+    RA inv_rho;
+};
+
+// Moments of the arrived (shifted) populations (prtlb_3d.py:428-433):
+// drho = sum h, J = rho u = sum e h + g/2 x.
+template <class L, class R, class RA, class H>
+__device__ __forceinline__ Moments<R, RA> moments(const H (&h)[L::Q], double half_g) {
+    Moments<R, RA> m;
+    RA s = RA(h[0]);
+    RA jx = RA(0), jy = RA(0), jz = RA(0);
+#pragma unroll
+    for (int p = 0; p < L::NP; ++p) {
+        const int a = L::pa(p), b = L::pb(p);
+        s += RA(h[a]) + RA(h[b]);
+        const RA d = RA(h[a]) - RA(h[b]);
+        if (L::c(a, 0) == 1) jx += d;
+        if (L::c(a, 0) == -1) jx -= d;
+        if (L::c(a, 1) == 1) jy += d;
+        if (L::c(a, 1) == -1) jy -= d;
+        if (L::c(a, 2) == 1) jz += d;
+        if (L::c(a, 2) == -1) jz -= d;
+    }
+    jx += RA(half_g);
+    m.jx = jx;
+    m.jy = jy;
+    m.jz = jz;
+    const RA rho = RA(1) + s;
+    m.inv_rho = RA(1) / rho;
+    m.drho = R(s);
+    m.jsq = R((jx * jx + jy * jy + jz * jz) * m.inv_rho);  // rho u^2 = |J|^2 / rho
+    return m;
+}
+
+// TRT collision (_trt_collide, prtlb_3d.py:142-154) + Guo forcing in the
+// shifted variables, written with J = rho u so that rho cancels in the
+// antisymmetric equilibrium (w rho 3 e.u = 3 w e.J) and rho u u = J J / rho in
+// the symmetric one.  The new population is h + delta with delta summed
+// first, so the stored result rounds once; it goes to slot i of voxel c.
+template <class L, class S, class R, class RA>
+__device__ __forceinline__ void collide_store(S* __restrict__ lw, int c, long long N,
+                                              const typename Pop<S>::H (&h)[L::Q],
+                                              const Moments<R, RA>& m, const LbParams& kc) {
+    const R omp = R(kc.omp);
+    const R inv_rho = R(m.inv_rho);
+    const R heq0 = R(L::w(0)) * (m.drho - R(1.5) * m.jsq);
+    const R h0 = R(h[0]);
+    Pop<S>::st(lw + c, h0 - omp * (h0 - heq0), kc.scale);
+#pragma unroll
+    for (int p = 0; p < L::NP; ++p) {
+        const int a = L::pa(p), b = L::pb(p);
+        RA eJ = RA(0);
+        if (L::c(a, 0) == 1) eJ += m.jx;
+        if (L::c(a, 0) == -1) eJ -= m.jx;
+        if (L::c(a, 1) == 1) eJ += m.jy;
+        if (L::c(a, 1) == -1) eJ -= m.jy;
+        if (L::c(a, 2) == 1) eJ += m.jz;
+        if (L::c(a, 2) == -1) eJ -= m.jz;
+        const R eJr = R(eJ);
+        const R heq_p = R(L::w(a)) * (m.drho + (R(4.5) * eJr * eJr * inv_rho - R(1.5) * m.jsq));
+        const R ha = R(h[a]), hb = R(h[b]);
+        const R dp = omp * (R(0.5) * (ha + hb) - heq_p);
+        const RA dma = RA(kc.omm) * (RA(0.5) * (RA(h[a]) - RA(h[b])) - RA(3.0 * L::w(a)) * eJ);
+        const R dm = R(dma);
+        const R gp = R(kc.guo[p]);
+        Pop<S>::st(lw + (long long)a * N + c, ha + ((gp - dp) - dm), kc.scale);
+        Pop<S>::st(lw + (long long)b * N + c, hb + ((dm - dp) - gp), kc.scale);
+    }
+}
+
+constexpr int kFlowThreads = 256;
+
+// One whole LB iteration t: lattice (t & 1) is read, lattice ((t + 1) & 1)
+// written; solid voxels do nothing.
+template <class L, class M, bool ODD, bool CHECK>
+__global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
+    lb_step_kernel(typename M::S* __restrict__ f, const uint32_t* __restrict__ nbmask, Grid g,
+                   LbParams kc, const FlowCtrl* __restrict__ ctrl, int kstep,
+                   double* __restrict__ partials) {
+    using S = typename M::S;
+    using R = typename M::R;
+    using RA = typename M::RA;
+    const long long it = ctrl->it_base + kstep;
+    if (ctrl->done || it >= ctrl->nit) return;  // uniform over the grid
+    const int c = blockIdx.x * kFlowThreads + threadIdx.x;
+    const long long QN = (long long)L::Q * g.n;
+    const S* lr = ODD ? f + QN : f;
+    S* lw = ODD ? f : f + QN;
+    double acc = 0.0;
+    if (c < g.n) {
+        const uint32_t nb = nbmask[c];
+        if (nb & kFluidBit) {
+            typename Pop<S>::H h[L::Q];
+            gather<L, S>(lr, lw, c, nb, g, g.n, kc.inv_scale, h);
+            const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
+            collide_store<L, S, R, RA>(lw, c, g.n, h, m, kc);
+            if (CHECK) acc = fabs((double)m.jx * (double)m.inv_rho);
+        }
+    }
+    if (CHECK) {
+        __shared__ double sh[kFlowThreads / 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double v = threadIdx.x < kFlowThreads / 32 ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (threadIdx.x == 0) partials[blockIdx.x] = v;
+        }
+    }
+}
+
+// Deterministic sum of per-block partials by one block.
+__device__ double block_sum_fixed(const double* __restrict__ p, int n) {
+    __shared__ double sh[256];
+    double v = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v += p[i];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// FlowConvergence.done() at the end of a chunk of `every` iterations
+// (prtlb_3d.py:220-235).  Also decides whether the while-graph goes on.
+__global__ void flow_check_kernel(FlowCtrl* ctrl, const double* __restrict__ partials, int nb,
+                                  cudaGraphConditionalHandle h, int use_handle) {
+    const int done_before = ctrl->done;
+    const long long base = ctrl->it_base;
+    const long long end = min(base + (long long)ctrl->every, ctrl->nit);
+    const bool full = (end - base) == ctrl->every;
+    double s = 0.0;
+    if (!done_before && full && ctrl->tol > 0) s = block_sum_fixed(partials, nb);
+    if (threadIdx.x != 0) return;
+    if (done_before) {
+        if (use_handle) cudaGraphSetConditional(h, 0);
+        return;
+    }
+    ctrl->iters = end;
+    if (ctrl->tol > 0 && full && (end % ctrl->every) == 0) {
+        const double u = ctrl->nfluid > 0 ? s / (double)ctrl->nfluid : 0.0;
+        if (ctrl->has_prev) {
+            ctrl->change = fabs(u - ctrl->prev) / fmax(fabs(u), 1e-30);
+            if (ctrl->change <= ctrl->tol) ctrl->converged = 1;
+        }
+        ctrl->prev = u;
+        ctrl->has_prev = 1;
+    }
+    ctrl->it_base = end;
+    if (ctrl->converged || end >= ctrl->nit) ctrl->done = 1;
+    if (use_handle) cudaGraphSetConditional(h, ctrl->done ? 0 : 1);
+}
+
+// Final field (prtlb_3d.py:451-456): v = (sum e f + g/2 x) / rho on pore
+// voxels, 0 in solid, cast to float32; plus FP64 reductions used by the
+// refusals of _checked_flow (prtlb_3d.py:267-316) and the permeability.
+// The state after `iters` iterations is gathered exactly as iteration
+// `iters` would gather it.
+// partials layout: 5 doubles per block: sum ux, sum rho, sum speed, max speed, nonfinite
+template <class L, class M, bool ODD>
+__global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
+    lb_moments_kernel(const typename M::S* __restrict__ f, const uint32_t* __restrict__ nbmask,
+                      Grid g, LbParams k, float* __restrict__ vel, double* __restrict__ partials) {
+    using S = typename M::S;
+    using R = typename M::R;
+    using RA = typename M::RA;
+    const int c = blockIdx.x * kFlowThreads + threadIdx.x;
+    const long long QN = (long long)L::Q * g.n;
+    const S* lr = ODD ? f + QN : f;
+    const S* lw = ODD ? f : f + QN;
+    double sux = 0.0, srho = 0.0, ssp = 0.0, mx = 0.0, nonf = 0.0;
+    if (c < g.n) {
+        float vx = 0.f, vy = 0.f, vz = 0.f;
+        const uint32_t nb = nbmask[c];
+        if (nb & kFluidBit) {
+            typename Pop<S>::H h[L::Q];
+            gather<L, S>(lr, lw, c, nb, g, g.n, k.inv_scale, h);
+            const Moments<R, RA> m = moments<L, R, RA>(h, k.half_g);
+            const RA ux = m.jx * m.inv_rho, uy = m.jy * m.inv_rho, uz = m.jz * m.inv_rho;
+            vx = (float)ux;
+            vy = (float)uy;
+            vz = (float)uz;
+            sux = (double)ux;
+            srho = 1.0 + (double)m.drho;
+            // speed the way _checked_flow computes it: float32, (x^2 + y^2) + z^2
+            const float sp = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)),
+                                             __fmul_rn(vz, vz)));
+            nonf = (float)(!isfinite(vx)) + (float)(!isfinite(vy)) + (float)(!isfinite(vz));
+            if (isfinite(sp)) {
+                ssp = sp;
+                mx = sp;
+            }
+        }
+        // 2D grids: the reference returns (ux, uy, 0); our y is the storage z
+        if (L::Q == 9) {
+            vel[c] = vx;
+            vel[g.n + c] = vz;
+            vel[2 * g.n + c] = 0.f;
+        } else {
+            vel[c] = vx;
+            vel[g.n + c] = vy;
+            vel[2 * g.n + c] = vz;
+        }
+    }
+    __shared__ double sh[5][kFlowThreads / 32];
+    double v[5] = {sux, srho, ssp, mx, nonf};
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double t = __shfl_down_sync(0xffffffffu, v[q], o);
+            v[q] = (q == 3) ? fmax(v[q], t) : v[q] + t;
+        }
+        if ((threadIdx.x & 31) == 0) sh[q][threadIdx.x >> 5] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            double t = threadIdx.x < kFlowThreads / 32 ? sh[q][threadIdx.x] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                double u = __shfl_down_sync(0xffffffffu, t, o);
+                t = (q == 3) ? fmax(t, u) : t + u;
+            }
+            if (threadIdx.x == 0) partials[(long long)blockIdx.x * 5 + q] = t;
+        }
+    }
+}
+
+__global__ void final_reduce_kernel(const double* __restrict__ partials, int nb, double* out) {
+    __shared__ double sh[5][256];
+    double v[5] = {0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            double t = partials[(long long)i * 5 + q];
+            v[q] = (q == 3) ? fmax(v[q], t) : v[q] + t;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) sh[q][threadIdx.x] = v[q];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                double a = sh[q][threadIdx.x], b = sh[q][threadIdx.x + s];
+                sh[q][threadIdx.x] = (q == 3) ? fmax(a, b) : a + b;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 5) out[threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// Per-voxel neighbour mask: kFluidBit for a pore voxel, bit i (1..Q-1) when
+// the upstream voxel x - e_i (periodic) is rock.
+template <class L>
+__global__ void nbmask_kernel(const uint8_t* __restrict__ mat, Grid g, int pore,
+                              uint32_t* __restrict__ nbmask) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= g.n) return;
+    const int z = (int)(c % g.nz);
+    const long long t = c / g.nz;
+    const int y = (int)(t % g.ny);
+    const int x = (int)(t / g.ny);
+    uint32_t m = (mat[c] == pore) ? kFluidBit : 0u;
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        int xx = x - L::c(i, 0), yy = y - L::c(i, 1), zz = z - L::c(i, 2);
+        xx = xx < 0 ? g.nx - 1 : (xx >= g.nx ? 0 : xx);
+        yy = yy < 0 ? g.ny - 1 : (yy >= g.ny ? 0 : yy);
+        zz = zz < 0 ? g.nz - 1 : (zz >= g.nz ? 0 : zz);
+        const long long s = ((long long)xx * g.ny + yy) * g.nz + zz;
+        if (mat[s] != pore) m |= 1u << i;
+    }
+    nbmask[c] = m;
+}
+
+// -------------------------------------------------------------------------
+// launchers
+// -------------------------------------------------------------------------
+int flow_blocks(const Grid& g) { return (int)((g.n + kFlowThreads - 1) / kFlowThreads); }
+
+template <class L, class M>
+static cudaError_t launch_step_t(bool odd, bool check, void* f, const uint32_t* nbm,
+                                 const Grid& g, const LbParams& k, const FlowCtrl* ctrl, int kstep,
+                                 double* partials, cudaStream_t s) {
+    dim3 grid(flow_blocks(g));
+    typename M::S* fs = static_cast<typename M::S*>(f);
+    if (!odd && !check) lb_step_kernel<L, M, false, false><<<grid, kFlowThreads, 0, s>>>(fs, nbm, g, k, ctrl, kstep, partials);
+    if (!odd && check) lb_step_kernel<L, M, false, true><<<grid, kFlowThreads, 0, s>>>(fs, nbm, g, k, ctrl, kstep, partials);
+    if (odd && !check) lb_step_kernel<L, M, true, false><<<grid, kFlowThreads, 0, s>>>(fs, nbm, g, k, ctrl, kstep, partials);
+    if (odd && check) lb_step_kernel<L, M, true, true><<<grid, kFlowThreads, 0, s>>>(fs, nbm, g, k, ctrl, kstep, partials);
+    return cudaGetLastError();
+}
+
+#define PRT_DISPATCH(FN, ...)                                                        \
+    if (nd == 3) {                                                                   \
+        if (precision == PRT_FP64) return FN<D3Q19, ModeF64>(__VA_ARGS__);           \
+        if (precision == PRT_FP32) return FN<D3Q19, ModeF32D>(__VA_ARGS__);          \
+        if (precision == PRT_FP32_F32) return FN<D3Q19, ModeF32>(__VA_ARGS__);       \
+        return FN<D3Q19, ModeF16>(__VA_ARGS__);                                      \
+    }                                                                                \
+    if (precision == PRT_FP64) return FN<D2Q9, ModeF64>(__VA_ARGS__);                \
+    if (precision == PRT_FP32) return FN<D2Q9, ModeF32D>(__VA_ARGS__);               \
+    if (precision == PRT_FP32_F32) return FN<D2Q9, ModeF32>(__VA_ARGS__);            \
+    return FN<D2Q9, ModeF16>(__VA_ARGS__);
+
+cudaError_t flow_launch_step(int nd, int precision, bool odd, bool check, void* f,
+                             const uint32_t* nbm, const Grid& g, const LbParams& k,
+                             const FlowCtrl* ctrl, int kstep, double* partials, cudaStream_t s) {
+    PRT_DISPATCH(launch_step_t, odd, check, f, nbm, g, k, ctrl, kstep, partials, s)
+}
+
+cudaError_t flow_launch_check(FlowCtrl* ctrl, const double* partials, int nblocks,
+                              cudaGraphConditionalHandle h, int use_handle, cudaStream_t s) {
+    flow_check_kernel<<<1, 256, 0, s>>>(ctrl, partials, nblocks, h, use_handle);
+    return cudaGetLastError();
+}
+
+template <class L, class M>
+static cudaError_t launch_moments_t(bool odd, const void* f, const uint32_t* nbm, const Grid& g,
+                                    const LbParams& k, float* vel, double* partials, cudaStream_t s) {
+    const typename M::S* fs = static_cast<const typename M::S*>(f);
+    if (odd) lb_moments_kernel<L, M, true><<<flow_blocks(g), kFlowThreads, 0, s>>>(fs, nbm, g, k, vel, partials);
+    else lb_moments_kernel<L, M, false><<<flow_blocks(g), kFlowThreads, 0, s>>>(fs, nbm, g, k, vel, partials);
+    return cudaGetLastError();
+}
+
+cudaError_t flow_launch_moments(int nd, int precision, bool odd, const void* f,
+                                const uint32_t* nbm, const Grid& g, const LbParams& k, float* vel,
+                                double* partials, cudaStream_t s) {
+    PRT_DISPATCH(launch_moments_t, odd, f, nbm, g, k, vel, partials, s)
+}
+
+cudaError_t flow_launch_nbmask(int nd, const uint8_t* mat, const Grid& g, int pore,
+                               uint32_t* nbmask, cudaStream_t s) {
+    const unsigned nb = (unsigned)((g.n + 255) / 256);
+    if (nd == 3) nbmask_kernel<D3Q19><<<nb, 256, 0, s>>>(mat, g, pore, nbmask);
+    else nbmask_kernel<D2Q9><<<nb, 256, 0, s>>>(mat, g, pore, nbmask);
+    return cudaGetLastError();
+}
+
+cudaError_t flow_launch_final_reduce(const double* partials, int nb, double* out, cudaStream_t s) {
+    final_reduce_kernel<<<1, 256, 0, s>>>(partials, nb, out);
+    return cudaGetLastError();
+}
+
+// compile-time checks of the lattice tables
+static_assert(D3Q19::opp(7) == 8 && D3Q19::opp(18) == 17, "D3Q19 opposites");
+static_assert(D3Q19::c(13, 0) == 1 && D3Q19::c(13, 2) == -1, "D3Q19 e_13");
+static_assert(D3Q19::c(18, 1) == -1 && D3Q19::c(18, 2) == 1, "D3Q19 e_18");
+static_assert(D2Q9::pa(0) == 1 && D2Q9::pb(0) == 3 && D2Q9::pa(3) == 6 && D2Q9::pb(3) == 8, "D2Q9 pairs");
+static_assert(D2Q9::opp(1) == 3 && D2Q9::opp(2) == 4 && D2Q9::opp(3) == 1 && D2Q9::opp(4) == 2 &&
+                  D2Q9::opp(5) == 7 && D2Q9::opp(6) == 8 && D2Q9::opp(7) == 5 && D2Q9::opp(8) == 6,
+              "D2Q9 opposites");
+static_assert(D2Q9::ex(6) == -1 && D2Q9::ey(6) == 1 && D2Q9::ex(8) == 1 && D2Q9::ey(8) == -1, "D2Q9 e");
+
+}  // namespace prt

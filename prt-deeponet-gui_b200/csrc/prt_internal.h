@@ -32,12 +32,13 @@ struct FlowCtrl {
     int converged;
 };
 
-template <class R>
-struct LbConst {
-    R omp, omm;   // omega+ , omega-
-    R half_g;     // force / 2, added to the x momentum
-    R guo[9];     // w_a (1 - omega-/2) 3 g c_ax for the first member of each pair
-    float scale;  // FP16 storage scale (2^k) and its inverse
+// Constants of one flow solve, in float64; kernels round them to their
+// arithmetic type.
+struct LbParams {
+    double omp, omm;  // omega+ , omega-
+    double half_g;    // force / 2, added to the x momentum
+    double guo[9];    // w_a (1 - omega-/2) 3 g c_ax for the first member of each pair
+    float scale;      // FP16 storage scale (2^k) and its inverse
     float inv_scale;
 };
 
@@ -100,19 +101,21 @@ struct PairTree {
     const int* level_off;  // nlevel + 1 offsets into the inner arrays
 };
 
-// Kernel launchers (flow.cu) ------------------------------------------------
-// Returns cudaSuccess or the launch error.
+// Kernel launchers (lb_flow.cu) ---------------------------------------------
+// Returns cudaSuccess or the launch error.  f holds the two lattices (read /
+// write swap with the iteration parity), Q * n populations each.
+constexpr uint32_t kFluidBit = 1u << 31;  // in the per-voxel neighbour mask
 cudaError_t flow_launch_step(int nd, int precision, bool odd, bool check, void* f,
-                             const uint8_t* fluid, const Grid& g, const void* lbconst,
+                             const uint32_t* nbmask, const Grid& g, const LbParams& lbp,
                              const FlowCtrl* ctrl, int kstep, double* partials,
                              cudaStream_t s);
 cudaError_t flow_launch_check(FlowCtrl* ctrl, const double* partials, int nblocks,
                               cudaGraphConditionalHandle h, int use_handle, cudaStream_t s);
 cudaError_t flow_launch_moments(int nd, int precision, bool odd, const void* f,
-                                const uint8_t* fluid, const Grid& g, const void* lbconst,
+                                const uint32_t* nbmask, const Grid& g, const LbParams& lbp,
                                 float* vel, double* partials, cudaStream_t s);
-cudaError_t flow_launch_fluid_mask(const uint8_t* mat, uint8_t* fluid, long long n,
-                                   int pore_code, cudaStream_t s);
+cudaError_t flow_launch_nbmask(int nd, const uint8_t* mat, const Grid& g, int pore,
+                               uint32_t* nbmask, cudaStream_t s);
 cudaError_t flow_launch_final_reduce(const double* partials, int nblocks, double* out,
                                      cudaStream_t s);
 int flow_blocks(const Grid& g);

@@ -205,10 +205,10 @@ cudaError_t build_while_graph(cudaStream_t s, GraphHolder& gh, Emit emit) {
     return e;
 }
 
-__global__ void count_fluid_kernel(const uint8_t* __restrict__ fluid, long long n,
+__global__ void count_fluid_kernel(const uint32_t* __restrict__ nbmask, long long n,
                                    unsigned long long* out) {
     long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int v = (c < n && fluid[c]) ? 1 : 0;
+    int v = (c < n && (nbmask[c] & kFluidBit)) ? 1 : 0;
     v = __syncthreads_count(v);
     if (threadIdx.x == 0 && v) atomicAdd(out, (unsigned long long)v);
 }
@@ -228,16 +228,15 @@ Grid make_grid(int nd, const int32_t* dims) {
     return g;
 }
 
-template <class R>
-void fill_lbconst(LbConst<R>& k, int nd, double force, double tau, double magic, float scale) {
+void fill_lbconst(LbParams& k, int nd, double force, double tau, double magic, float scale) {
     // _trt_minus (prtlb_3d.py:130-139)
     const double om_p = 1.0 / tau;
     const double lam_p = 1.0 / om_p - 0.5;
     const double om_m = 1.0 / (magic / lam_p + 0.5);
-    k.omp = (R)om_p;
-    k.omm = (R)om_m;
-    k.half_g = (R)(0.5 * force);
-    for (int p = 0; p < 9; ++p) k.guo[p] = (R)0;
+    k.omp = om_p;
+    k.omm = om_m;
+    k.half_g = 0.5 * force;
+    for (int p = 0; p < 9; ++p) k.guo[p] = 0.0;
     // first member of each pair and its x component
     if (nd == 3) {
         // pairs (1,2) (3,4) ... (17,18); e_x of 1,7,9,11,13 is +1, of 3,5,15,17 is 0
@@ -246,7 +245,7 @@ void fill_lbconst(LbConst<R>& k, int nd, double force, double tau, double magic,
         for (int p = 0; p < 9; ++p) {
             const int a = pa[p];
             const double w = a < 7 ? 1.0 / 18.0 : 1.0 / 36.0;
-            k.guo[p] = (R)(w * (1 - 0.5 * om_m) * 3.0 * force * ex[a]);
+            k.guo[p] = w * (1 - 0.5 * om_m) * 3.0 * force * ex[a];
         }
     } else {
         const int pa[4] = {1, 2, 5, 6};
@@ -254,7 +253,7 @@ void fill_lbconst(LbConst<R>& k, int nd, double force, double tau, double magic,
         for (int p = 0; p < 4; ++p) {
             const int a = pa[p];
             const double w = a < 5 ? 1.0 / 9.0 : 1.0 / 36.0;
-            k.guo[p] = (R)(w * (1 - 0.5 * om_m) * 3.0 * force * ex[a]);
+            k.guo[p] = w * (1 - 0.5 * om_m) * 3.0 * force * ex[a];
         }
     }
     k.scale = scale;
@@ -354,7 +353,7 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
                     "solver cannot run.");
     if (p->every <= 0 || (p->every & 1))
         return fail(ctx, PRT_E_INVALID, "the convergence interval must be a positive even number");
-    if (p->precision < PRT_FP64 || p->precision > PRT_FP16)
+    if (p->precision < PRT_FP64 || p->precision > PRT_FP32_F32)
         return fail(ctx, PRT_E_INVALID, "unknown precision");
     if (p->nit < 0) return fail(ctx, PRT_E_INVALID, "negative iteration cap");
     CK(cudaSetDevice(ctx->device));
@@ -362,28 +361,30 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
     FlowState& F = ctx->flow;
     const Grid g = make_grid(p->nd, p->dims);
     const int Q = p->nd == 3 ? 19 : 9;
-    const size_t es = p->precision == PRT_FP64 ? 8 : (p->precision == PRT_FP32 ? 4 : 2);
+    const size_t es = p->precision == PRT_FP64 ? 8 : (p->precision == PRT_FP16 ? 2 : 4);
+    if (g.n >= (1ll << 31))
+        return fail(ctx, PRT_E_INVALID, "grids of 2^31 voxels or more are not supported");
     const int nb = flow_blocks(g);
-    CK(F.f.ensure((size_t)Q * g.n * es));
-    CK(F.fluid.ensure((size_t)g.n));
+    CK(F.f.ensure((size_t)2 * Q * g.n * es));  // two lattices
+    CK(F.fluid.ensure((size_t)g.n * 4));        // neighbour masks
     CK(F.partials.ensure((size_t)nb * 5 * sizeof(double)));
     CK(F.ctrl.ensure(sizeof(FlowCtrl)));
     CK(F.out5.ensure(8 * sizeof(double)));
     CK(F.count.ensure(sizeof(unsigned long long)));
 
-    // pore mask and its size
-    CK(flow_launch_fluid_mask(d_mat, F.fluid.as<uint8_t>(), g.n, 2, s));
+    // neighbour masks and the pore voxel count
+    CK(flow_launch_nbmask(p->nd, d_mat, g, 2, F.fluid.as<uint32_t>(), s));
     CK(cudaMemsetAsync(F.count.p, 0, sizeof(unsigned long long), s));
     count_fluid_kernel<<<(unsigned)((g.n + 255) / 256), 256, 0, s>>>(
-        F.fluid.as<uint8_t>(), g.n, F.count.as<unsigned long long>());
+        F.fluid.as<uint32_t>(), g.n, F.count.as<unsigned long long>());
     CK(cudaGetLastError());
     ctx->launches += 2;
     unsigned long long nfluid = 0;
     CK(cudaMemcpyAsync(&nfluid, F.count.p, sizeof(nfluid), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
 
-    // f = w_i everywhere: shifted storage h = 0
-    CK(cudaMemsetAsync(F.f.p, 0, (size_t)Q * g.n * es, s));
+    // f = w_i everywhere, in both lattices: shifted storage h = 0
+    CK(cudaMemsetAsync(F.f.p, 0, (size_t)2 * Q * g.n * es, s));
     FlowCtrl hc{};
     hc.it_base = 0;
     hc.nit = p->nit;
@@ -401,12 +402,8 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
         const double g0 = std::fabs(p->force) > 0 ? std::fabs(p->force) : 1e-6;
         scale = (float)std::ldexp(1.0, (int)std::floor(std::log2(1.0 / g0)));
     }
-    LbConst<double> kd;
-    LbConst<float> kf;
-    fill_lbconst(kd, p->nd, p->force, p->tau, p->magic, scale);
-    fill_lbconst(kf, p->nd, p->force, p->tau, p->magic, scale);
-    // float64 and float32 storage collide in float64; float16 storage in float32
-    const void* kc = p->precision == PRT_FP16 ? (const void*)&kf : (const void*)&kd;
+    LbParams kc;
+    fill_lbconst(kc, p->nd, p->force, p->tau, p->magic, scale);
 
     FlowCtrl* dctrl = F.ctrl.as<FlowCtrl>();
     double* parts = F.partials.as<double>();
@@ -414,7 +411,7 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
     auto emit = [&](cudaGraphConditionalHandle h, int use) -> cudaError_t {
         for (int k = 0; k < every; ++k) {
             cudaError_t e = flow_launch_step(p->nd, p->precision, (k & 1) != 0, k == every - 1,
-                                             F.f.p, F.fluid.as<uint8_t>(), g, kc, dctrl, k, parts, s);
+                                             F.f.p, F.fluid.as<uint32_t>(), g, kc, dctrl, k, parts, s);
             if (e != cudaSuccess) return e;
         }
         return flow_launch_check(dctrl, parts, nb, h, use, s);
@@ -471,7 +468,7 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
         ctx->timing[1] = (double)res.iters;
     }
     // final field from the state after `iters` iterations
-    CK(flow_launch_moments(p->nd, p->precision, (res.iters & 1) != 0, F.f.p, F.fluid.as<uint8_t>(),
+    CK(flow_launch_moments(p->nd, p->precision, (res.iters & 1) != 0, F.f.p, F.fluid.as<uint32_t>(),
                            g, kc, d_vel, parts, s));
     CK(flow_launch_final_reduce(parts, nb, F.out5.as<double>(), s));
     ctx->launches += 2;

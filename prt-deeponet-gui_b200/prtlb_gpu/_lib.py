@@ -25,8 +25,9 @@ PRT_E_NODEV = -6
 PRT_FP64 = 0
 PRT_FP32 = 1
 PRT_FP16 = 2
+PRT_FP32_F32 = 3
 
-PRECISIONS = {"fp64": PRT_FP64, "fp32": PRT_FP32, "fp16": PRT_FP16}
+PRECISIONS = {"fp64": PRT_FP64, "fp32": PRT_FP32, "fp16": PRT_FP16, "fp32f": PRT_FP32_F32}
 
 c_i32, c_u32, c_i64, c_f32, c_f64 = (ctypes.c_int32, ctypes.c_uint32, ctypes.c_int64,
                                      ctypes.c_float, ctypes.c_double)

@@ -7,10 +7,11 @@ The solve itself runs in libprtlb.so: one CUDA graph per solve whose body is
 50 fused stream-collide iterations plus the convergence check.
 
 Keyword-only additions: ``precision`` ("fp64" default = the reference's
-arithmetic; "fp32" stores f_i - w_i in float32 and collides in float64, so
-only the store rounds; "fp16" stores it scaled by 2^k in float16 and collides
-in float32), ``device`` (CUDA ordinal) and ``ctx`` (an explicit
-``prtlb_gpu.Context``).
+arithmetic; "fp32" stores f_i - w_i in float32 and forms the momentum and
+the antisymmetric non-equilibrium part in float64, the rest in float32;
+"fp32f" does all of the collision in float32; "fp16" stores f_i - w_i scaled
+by 2^k in float16 and collides in float32), ``device`` (CUDA ordinal) and
+``ctx`` (an explicit ``prtlb_gpu.Context``).
 """
 
 import ctypes
