@@ -62,7 +62,8 @@ int prt_create(int device, prt_ctx** out);
 /* Release every device buffer of the context and the context itself. */
 void prt_destroy(prt_ctx* ctx);
 
-/* Message of the last failed call on ctx (ctx == NULL: last prt_create). */
+/* Message of the last failed call on ctx (ctx == NULL: the last failed call
+ * without a context on this thread, prt_create or prt_flow_noalloc). */
 const char* prt_last_error(const prt_ctx* ctx);
 
 /* Number of kernels this context has launched so far (graph nodes included). */
@@ -127,6 +128,24 @@ int prt_flow(prt_ctx* ctx, const uint8_t* mat, const prt_flow_params* p,
 /* Same, with DEVICE pointers (already resident on the context's device). */
 int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p,
                  float* d_vel_out, prt_flow_info* info);
+
+/* The flow solve for callers that cannot allocate device memory.  No
+ * counterpart in the reference: it exists for hosts that own the device
+ * memory pool (a framework that forbids foreign cudaMalloc, a real-time loop
+ * that must not block on the allocator, a plug-in host that hands out
+ * buffers but no allocator).  The caller passes d_mat and d_vel_out as
+ * device pointers it owns and a cudaStream_t (NULL: the default stream); no
+ * context is needed and nothing is allocated or freed.  All other scratch
+ * (both lattices, masks, partial sums, control block) is one 48 MiB
+ * file-scope __device__ array in the library, which every GPU that loads
+ * the library holds until exit; a grid that does not fit (64^3 D3Q19 at
+ * float32 does) is refused with PRT_E_INVALID and a message giving both
+ * sizes.  The first call on a device looks up the array's address; make it
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race and must be serialised.  Runs on the current device; errors
+ * are read with prt_last_error(NULL). */
+int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, float* d_vel_out,
+                     prt_flow_info* info, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Transport: solve_adr (prtlb_3d.py:781-1595)                              */

@@ -1,0 +1,240 @@
+// noalloc.cu -- prt_flow_noalloc: the flow solve with no device allocation.
+//
+// Who needs it: callers that cannot call cudaMalloc -- code running inside a
+// host framework that owns the whole device pool (and forbids foreign
+// allocations), real-time loops that must never block on the allocator, and
+// plug-in hosts that hand out device buffers for inputs and outputs but no
+// allocator.  They pass the material grid and the velocity output as device
+// pointers they already own, plus a stream; every other byte the solve needs
+// (both population lattices, the neighbour masks, the per-block partial sums
+// and the control block) lives in one file-scope __device__ array compiled
+// into the library.
+//
+// Limits and sharing:
+//   - The array is kNoAllocScratchBytes (48 MiB) on every GPU that loads the
+//     library, held until the process exits.  A grid whose scratch would not
+//     fit is refused with PRT_E_INVALID and a message giving both sizes; 64^3
+//     D3Q19 with float32 populations fits.
+//   - All calls on one device share the array and it keeps the last call's
+//     contents; each call clears what must start at zero (the lattices, the
+//     pore count) itself.  Calls whose work overlaps on the GPU (different
+//     streams or threads at the same time) race on the array and give wrong
+//     results: serialise them.
+//   - The first call on a device looks up the array's device address
+//     (cudaGetSymbolAddress, with that device current) and caches it; make
+//     that first call before any stream capture.
+//   - The solve runs on the calling thread's current device.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "prt_internal.h"
+
+using namespace prt;
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 48u << 20;
+constexpr int kMaxDevices = 64;
+
+// The scratch itself.  In host code this name is only a stand-in for the
+// device symbol; the kernels get the address from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_scratch[kNoAllocScratchBytes];
+
+std::mutex g_mu;
+void* g_addr[kMaxDevices] = {nullptr};
+
+// the message goes where prt_last_error(NULL) reads it
+int fail(int code, const std::string& msg) {
+    prt::set_noctx_error(msg.c_str());
+    return code;
+}
+
+size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Device address of g_scratch on the current device, looked up once.
+cudaError_t scratch_addr(int dev, void** out) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+        if (e != cudaSuccess) return e;
+        g_addr[dev] = p;
+    }
+    *out = g_addr[dev];
+    return cudaSuccess;
+}
+
+__global__ void noalloc_count_kernel(const uint32_t* __restrict__ nbmask, long long n,
+                                     unsigned long long* out) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int v = (c < n && (nbmask[c] & kFluidBit)) ? 1 : 0;
+    v = __syncthreads_count(v);
+    if (threadIdx.x == 0 && v) atomicAdd(out, (unsigned long long)v);
+}
+
+__global__ void noalloc_ctrl_kernel(FlowCtrl* ctrl, const unsigned long long* count, long long nit,
+                                    double tol, int every) {
+    // control block of a fresh solve; the pore count comes from the device
+    ctrl->it_base = 0;
+    ctrl->nit = nit;
+    ctrl->iters = 0;
+    ctrl->nfluid = (long long)*count;
+    ctrl->tol = tol;
+    ctrl->prev = 0.0;
+    ctrl->change = INFINITY;
+    ctrl->every = every;
+    ctrl->done = nit == 0 ? 1 : 0;
+    ctrl->has_prev = 0;
+    ctrl->converged = 0;
+}
+
+}  // namespace
+
+#define NCK(expr)                                                                      \
+    do {                                                                               \
+        cudaError_t _e = (expr);                                                       \
+        if (_e != cudaSuccess)                                                         \
+            return fail(_e == cudaErrorMemoryAllocation ? PRT_E_OOM : PRT_E_CUDA,      \
+                        std::string(#expr) + ": " + cudaGetErrorString(_e));           \
+    } while (0)
+
+extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, float* d_vel_out,
+                                prt_flow_info* info, void* stream) {
+    if (!p || !d_mat || !d_vel_out) return fail(PRT_E_INVALID, "null argument");
+    if (p->nd != 2 && p->nd != 3) return fail(PRT_E_INVALID, "nd must be 2 or 3");
+    for (int i = 0; i < p->nd; ++i)
+        if (p->dims[i] <= 0) return fail(PRT_E_INVALID, "grid dimensions must be positive");
+    if (!(p->tau > 0.5))
+        return fail(PRT_E_INVALID, "tau must exceed 0.5; the viscosity (tau-1/2)/3 is negative "
+                                   "below it and the solver cannot run.");
+    if (p->every <= 0 || (p->every & 1))
+        return fail(PRT_E_INVALID, "the convergence interval must be a positive even number");
+    if (p->precision < PRT_FP64 || p->precision > PRT_FP32_F32)
+        return fail(PRT_E_INVALID, "unknown precision");
+    if (p->nit < 0) return fail(PRT_E_INVALID, "negative iteration cap");
+    Grid g;
+    g.nx = p->dims[0];
+    g.ny = p->nd == 3 ? p->dims[1] : 1;
+    g.nz = p->nd == 3 ? p->dims[2] : p->dims[1];
+    g.n = (long long)g.nx * g.ny * g.nz;
+    if (g.n >= (1ll << 31)) return fail(PRT_E_INVALID, "grid too large");
+    const int Q = p->nd == 3 ? 19 : 9;
+    const size_t es = p->precision == PRT_FP64 ? 8 : (p->precision == PRT_FP16 ? 2 : 4);
+    const int nb = flow_blocks(g);
+    // scratch layout: control | count | 5 reduced sums | partials | masks | 2 lattices
+    const size_t o_ctrl = 0;
+    const size_t o_count = o_ctrl + up256(sizeof(FlowCtrl));
+    const size_t o_out5 = o_count + 256;
+    const size_t o_part = o_out5 + 256;
+    const size_t o_mask = o_part + up256((size_t)nb * 5 * sizeof(double));
+    const size_t o_lat = o_mask + up256((size_t)g.n * 4);
+    const size_t lat_bytes = (size_t)2 * Q * g.n * es;
+    const size_t need = o_lat + lat_bytes;
+    if (need > kNoAllocScratchBytes)
+        return fail(PRT_E_INVALID,
+                    "this grid needs " + std::to_string(need) + " bytes of scratch but the "
+                    "allocation-free solve has " + std::to_string(kNoAllocScratchBytes) +
+                    "; use prt_flow / prt_flow_dev");
+    int dev = 0;
+    NCK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(PRT_E_INVALID, "device ordinal too large");
+    void* base = nullptr;
+    NCK(scratch_addr(dev, &base));
+    unsigned char* sb = static_cast<unsigned char*>(base);
+    FlowCtrl* ctrl = reinterpret_cast<FlowCtrl*>(sb + o_ctrl);
+    unsigned long long* count = reinterpret_cast<unsigned long long*>(sb + o_count);
+    double* out5 = reinterpret_cast<double*>(sb + o_out5);
+    double* parts = reinterpret_cast<double*>(sb + o_part);
+    uint32_t* nbmask = reinterpret_cast<uint32_t*>(sb + o_mask);
+    void* f = sb + o_lat;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    // constants (_trt_minus, prtlb_3d.py:130-139; Guo term prtlb_3d.py:439-440)
+    LbParams k;
+    const double om_p = 1.0 / p->tau;
+    const double om_m = 1.0 / (p->magic / (1.0 / om_p - 0.5) + 0.5);
+    k.omp = om_p;
+    k.omm = om_m;
+    k.half_g = 0.5 * p->force;
+    for (int i = 0; i < 9; ++i) k.guo[i] = 0.0;
+    if (p->nd == 3) {
+        const int pa[9] = {1, 3, 5, 7, 9, 11, 13, 15, 17};
+        const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+        for (int i = 0; i < 9; ++i) {
+            const double w = pa[i] < 7 ? 1.0 / 18.0 : 1.0 / 36.0;
+            k.guo[i] = w * (1 - 0.5 * om_m) * 3.0 * p->force * ex[pa[i]];
+        }
+    } else {
+        const int pa[4] = {1, 2, 5, 6};
+        const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+        for (int i = 0; i < 4; ++i) {
+            const double w = pa[i] < 5 ? 1.0 / 9.0 : 1.0 / 36.0;
+            k.guo[i] = w * (1 - 0.5 * om_m) * 3.0 * p->force * ex[pa[i]];
+        }
+    }
+    float scale = 1.f;
+    if (p->precision == PRT_FP16) {
+        const double g0 = std::fabs(p->force) > 0 ? std::fabs(p->force) : 1e-6;
+        scale = (float)std::ldexp(1.0, (int)std::floor(std::log2(1.0 / g0)));
+    }
+    k.scale = scale;
+    k.inv_scale = 1.0f / scale;
+
+    // everything that must start at zero is cleared here: the array keeps
+    // whatever the previous call left
+    NCK(cudaMemsetAsync(f, 0, lat_bytes, s));
+    NCK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), s));
+    NCK(flow_launch_nbmask(p->nd, d_mat, g, 2, nbmask, s));
+    noalloc_count_kernel<<<(unsigned)((g.n + 255) / 256), 256, 0, s>>>(nbmask, g.n, count);
+    NCK(cudaGetLastError());
+    noalloc_ctrl_kernel<<<1, 1, 0, s>>>(ctrl, count, p->nit, p->tol, p->every);
+    NCK(cudaGetLastError());
+
+    // the time loop, launched directly (no graph objects), chunk by chunk;
+    // kernels after the stop are no-ops, so a few chunks go out per check
+    const long long chunks = (p->nit + p->every - 1) / p->every;
+    long long launched = 0;
+    FlowCtrl hc;
+    memset(&hc, 0, sizeof(hc));
+    hc.done = p->nit == 0 ? 1 : 0;
+    while (!hc.done && launched < chunks) {
+        for (int r = 0; r < 8 && launched < chunks; ++r, ++launched) {
+            for (int kk = 0; kk < p->every; ++kk)
+                NCK(flow_launch_step(p->nd, p->precision, (kk & 1) != 0, kk == p->every - 1, f,
+                                     nbmask, g, k, ctrl, kk, parts, s));
+            NCK(flow_launch_check(ctrl, parts, nb, cudaGraphConditionalHandle(0), 0, s));
+        }
+        NCK(cudaMemcpyAsync(&hc, ctrl, sizeof(hc), cudaMemcpyDeviceToHost, s));
+        NCK(cudaStreamSynchronize(s));
+    }
+    NCK(cudaMemcpyAsync(&hc, ctrl, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    NCK(cudaStreamSynchronize(s));
+    NCK(flow_launch_moments(p->nd, p->precision, (hc.iters & 1) != 0, f, nbmask, g, k, d_vel_out,
+                            parts, s));
+    NCK(flow_launch_final_reduce(parts, nb, out5, s));
+    double o5[5];
+    unsigned long long nfluid = 0;
+    NCK(cudaMemcpyAsync(o5, out5, sizeof(o5), cudaMemcpyDeviceToHost, s));
+    NCK(cudaMemcpyAsync(&nfluid, count, sizeof(nfluid), cudaMemcpyDeviceToHost, s));
+    NCK(cudaStreamSynchronize(s));
+    if (info) {
+        memset(info, 0, sizeof(*info));
+        info->iters = hc.iters;
+        info->converged = hc.converged;
+        info->change = hc.change;
+        info->fluid_cells = (int64_t)nfluid;
+        info->ux_sum = o5[0];
+        info->mass = o5[1];
+        info->speed_sum = o5[2];
+        info->umax = o5[3];
+        info->nonfinite = (int64_t)llround(o5[4]);
+        const double nu = (p->tau - 0.5) / 3.0;
+        info->permeability = p->force != 0 ? nu * (o5[0] / (double)g.n) / p->force : 0.0;
+        info->fp16_scale = scale;
+    }
+    return PRT_OK;
+}

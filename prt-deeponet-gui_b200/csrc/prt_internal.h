@@ -120,6 +120,9 @@ cudaError_t flow_launch_final_reduce(const double* partials, int nblocks, double
                                      cudaStream_t s);
 int flow_blocks(const Grid& g);
 
+// Sets what prt_last_error(NULL) returns on the calling thread (runtime.cu).
+void set_noctx_error(const char* msg);
+
 // Kernel launchers (adr.cu) -------------------------------------------------
 struct AdrDev {
     Grid g;

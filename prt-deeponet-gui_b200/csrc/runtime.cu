@@ -315,6 +315,9 @@ extern "C" const char* prt_last_error(const prt_ctx* c) {
     return c ? c->err.c_str() : g_create_error.c_str();
 }
 
+// Message of a failed call that has no context (prt_flow_noalloc).
+void prt::set_noctx_error(const char* msg) { g_create_error = msg ? msg : ""; }
+
 extern "C" int64_t prt_kernel_launches(const prt_ctx* c) { return c ? c->launches : 0; }
 
 extern "C" void* prt_stream(const prt_ctx* c) { return c ? (void*)c->stream : nullptr; }

@@ -96,6 +96,9 @@ _PROTOS = {
                                 ctypes.c_void_p, ctypes.POINTER(FlowInfo)]),
     "prt_flow_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(FlowParams),
                                     ctypes.c_void_p, ctypes.POINTER(FlowInfo)]),
+    "prt_flow_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FlowParams),
+                                        ctypes.c_void_p, ctypes.POINTER(FlowInfo),
+                                        ctypes.c_void_p]),
     "prt_adr_stage": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                      ctypes.POINTER(AdrGeom), ctypes.POINTER(AdrStats)]),
     "prt_adr_stage_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
