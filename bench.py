@@ -56,6 +56,10 @@ EDGE = 64
 POROSITY = 0.45
 SEED = 0
 FORCE, TAU, FLOW_TOL, FLOW_NIT = 2e-6, 0.8, 1e-6, 30000
+ADR_STEPS = None  # None: run to the reference's stop rule
+# DRAM bytes (read + write) of one lb_step_kernel launch from an ncu capture,
+# by grid edge (profiles/lb_step_kernel_plain3d.md); None until captured
+TRAFFIC_PER_LAUNCH = {64: 35480000}
 PE, DA, KS, N_T = 10.0, 1.0, 0.5, 5
 METRIC = "D3Q19 TRT+ADR GLUPS"
 UNIT = "GLUPS"
@@ -167,7 +171,7 @@ def device_solve(ctx, L, d_mat, d_vel, d_out, shape, chem):
     ctx.check(L.prt_adr_stage_dev(ctx.handle, ctypes.c_void_p(d_mat), ctypes.c_void_p(d_vel),
                                   ctypes.byref(geom), ctypes.byref(st)))
     S = prepare(shape, stats_dict(st), PE, DA, n_species=1, chem=chem)
-    steps = _run_device(ctx, S, N_T, d_out)
+    steps = _run_device(ctx, S, N_T, d_out, steps=ADR_STEPS)
     return int(fi.iters), int(steps)
 
 
@@ -242,7 +246,8 @@ def run_ours(args, rank, world, torch, dist):
             e0.record(stream)
             v = stokes_d3q19(g, nit=FLOW_NIT, force=FORCE, tau_lb=TAU, tol=FLOW_TOL,
                              precision="fp32", ctx=ctx)
-            out, tn = solve_adr(g, v, pe=PE, da=DA, n_t=N_T, n_species=1, chem=chem, ctx=ctx)
+            out, tn = solve_adr(g, v, pe=PE, da=DA, n_t=N_T, n_species=1, chem=chem, ctx=ctx,
+                                steps=ADR_STEPS)
             e1.record(stream)
             e1.synchronize()
             e2e_ms.append(e0.elapsed_time(e1))
@@ -255,15 +260,16 @@ def run_ours(args, rank, world, torch, dist):
     fl_ms = statistics.mean(flow_ms)
     ad_ms = statistics.mean(adr_ms)
     per_launch_ms = fl_ms / max(iters[0], 1)
-    lb_bytes = nfluid * LB_BYTES_PER_FLUID + ncell
+    lb_bytes = nfluid * LB_BYTES_PER_FLUID + 4 * ncell
     achieved = lb_bytes / (per_launch_ms * 1e-3) / 1e9
     peak, kind = peaks()
-    roof = {"kernel": "lb_step_kernel<D3Q19,float,double>", "bound": "hbm",
+    roof = {"kernel": "lb_step_kernel<D3Q19,ModeF32D>", "bound": "hbm",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": kind,
-            "bytes_per_launch": lb_bytes, "traffic": None,
-            "note": "per-launch time = flow loop events / iterations (includes graph "
-                    "launch gaps and the convergence check); 64^3 state (20 MB) is L2-resident"}
+            "bytes_per_launch": lb_bytes, "traffic": TRAFFIC_PER_LAUNCH.get(EDGE),
+            "note": "algorithmic bytes = 152 B per pore voxel (19 float32 read + written) + "
+                    "4 B neighbour mask per voxel; per-launch time = flow loop events / "
+                    "iterations (includes graph node gaps and the convergence check)"}
     res = {"ms_per_step": total_ms / args.steps, "value": value, "e2e": e2e_value,
            "h2d": h2d, "d2h": d2h, "launches": launches, "roof": roof, "clocks": clk.summary(),
            "flow_ms": fl_ms, "adr_ms": ad_ms, "iters": iters[0], "adr_steps": nsteps[0],
@@ -319,7 +325,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-its", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=100)
+    # smaller cases of the same kernels, for profiling runs only (the bench
+    # line is always taken with the defaults)
+    ap.add_argument("--edge", type=int, default=64)
+    ap.add_argument("--flow-nit", type=int, default=30000)
+    ap.add_argument("--adr-steps", type=int, default=None)
     args = ap.parse_args()
+    globals().update(EDGE=args.edge, FLOW_NIT=args.flow_nit, ADR_STEPS=args.adr_steps)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     config = {"workload": WORKLOAD, "edge": EDGE, "voxels": EDGE ** 3, "porosity": POROSITY,
