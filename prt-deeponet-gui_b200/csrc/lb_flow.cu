@@ -141,30 +141,35 @@ struct ModeF16 {  // scaled float16 populations, float32 collision
     static constexpr int min_blocks = 3;
 };
 
-// Gather the arrived populations of pore voxel c (see the file comment).
-// nb: bit i set when the upstream voxel c - e_i is rock.
+// Gather the arrived populations of pore voxel number k (see the file
+// comment).  Lattices hold the pore voxels only, in C order: voxel
+// cells[k] is slot k, and imap[voxel] is the slot of a pore voxel or -1.
 template <class L, class S>
-__device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __restrict__ lw, int c,
-                                       uint32_t nb, const Grid& g, long long N, float inv,
+__device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __restrict__ lw, int k,
+                                       const FlowMap& fm, const Grid& g, float inv,
                                        typename Pop<S>::H (&h)[L::Q]) {
-    const int z = c % g.nz;
-    const int t = c / g.nz;
+    const long long NF = fm.nf;
+    const int v = fm.cells[k];
+    const int z = v % g.nz;
+    const int t = v / g.nz;
     const int y = t % g.ny;
     const int x = t / g.ny;
     const int syz = g.ny * g.nz;
-    h[0] = Pop<S>::ld(lr + c, inv);
+    int src[L::Q];
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
-        if (nb & (1u << i)) {
-            h[i] = Pop<S>::ld(lw + (long long)L::opp(i) * N + c, inv);
-        } else {
-            const int dx = -L::c(i, 0), dy = -L::c(i, 1), dz = -L::c(i, 2);
-            int xx = x + dx, yy = y + dy, zz = z + dz;
-            if (dx) xx = xx < 0 ? g.nx - 1 : (xx >= g.nx ? 0 : xx);
-            if (dy) yy = yy < 0 ? g.ny - 1 : (yy >= g.ny ? 0 : yy);
-            if (dz) zz = zz < 0 ? g.nz - 1 : (zz >= g.nz ? 0 : zz);
-            h[i] = Pop<S>::ld(lr + (long long)i * N + (xx * syz + yy * g.nz + zz), inv);
-        }
+        const int dx = -L::c(i, 0), dy = -L::c(i, 1), dz = -L::c(i, 2);
+        int xx = x + dx, yy = y + dy, zz = z + dz;
+        if (dx) xx = xx < 0 ? g.nx - 1 : (xx >= g.nx ? 0 : xx);
+        if (dy) yy = yy < 0 ? g.ny - 1 : (yy >= g.ny ? 0 : yy);
+        if (dz) zz = zz < 0 ? g.nz - 1 : (zz >= g.nz ? 0 : zz);
+        src[i] = fm.imap[xx * syz + yy * g.nz + zz];
+    }
+    h[0] = Pop<S>::ld(lr + k, inv);
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        h[i] = src[i] >= 0 ? Pop<S>::ld(lr + (long long)i * NF + src[i], inv)
+                           : Pop<S>::ld(lw + (long long)L::opp(i) * NF + k, inv);
     }
 }
 
@@ -247,28 +252,24 @@ constexpr int kFlowThreads = 256;
 // written; solid voxels do nothing.
 template <class L, class M, bool ODD, bool CHECK>
 __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
-    lb_step_kernel(typename M::S* __restrict__ f, const uint32_t* __restrict__ nbmask, Grid g,
-                   LbParams kc, const FlowCtrl* __restrict__ ctrl, int kstep,
-                   double* __restrict__ partials) {
+    lb_step_kernel(typename M::S* __restrict__ f, FlowMap fm, Grid g, LbParams kc,
+                   const FlowCtrl* __restrict__ ctrl, int kstep, double* __restrict__ partials) {
     using S = typename M::S;
     using R = typename M::R;
     using RA = typename M::RA;
     const long long it = ctrl->it_base + kstep;
     if (ctrl->done || it >= ctrl->nit) return;  // uniform over the grid
-    const int c = blockIdx.x * kFlowThreads + threadIdx.x;
-    const long long QN = (long long)L::Q * g.n;
+    const int k = blockIdx.x * kFlowThreads + threadIdx.x;
+    const long long QN = (long long)L::Q * fm.nf;
     const S* lr = ODD ? f + QN : f;
     S* lw = ODD ? f : f + QN;
     double acc = 0.0;
-    if (c < g.n) {
-        const uint32_t nb = nbmask[c];
-        if (nb & kFluidBit) {
-            typename Pop<S>::H h[L::Q];
-            gather<L, S>(lr, lw, c, nb, g, g.n, kc.inv_scale, h);
-            const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
-            collide_store<L, S, R, RA>(lw, c, g.n, h, m, kc);
-            if (CHECK) acc = fabs((double)m.jx * (double)m.inv_rho);
-        }
+    if (k < fm.nf) {
+        typename Pop<S>::H h[L::Q];
+        gather<L, S>(lr, lw, k, fm, g, kc.inv_scale, h);
+        const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
+        collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
+        if (CHECK) acc = fabs((double)m.jx * (double)m.inv_rho);
     }
     if (CHECK) {
         __shared__ double sh[kFlowThreads / 32];
@@ -339,22 +340,23 @@ __global__ void flow_check_kernel(FlowCtrl* ctrl, const double* __restrict__ par
 // partials layout: 5 doubles per block: sum ux, sum rho, sum speed, max speed, nonfinite
 template <class L, class M, bool ODD>
 __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
-    lb_moments_kernel(const typename M::S* __restrict__ f, const uint32_t* __restrict__ nbmask,
-                      Grid g, LbParams k, float* __restrict__ vel, double* __restrict__ partials) {
+    lb_moments_kernel(const typename M::S* __restrict__ f, FlowMap fm, Grid g, LbParams k,
+                      float* __restrict__ vel, double* __restrict__ partials) {
     using S = typename M::S;
     using R = typename M::R;
     using RA = typename M::RA;
-    const int c = blockIdx.x * kFlowThreads + threadIdx.x;
-    const long long QN = (long long)L::Q * g.n;
+    const int kk = blockIdx.x * kFlowThreads + threadIdx.x;
+    const long long QN = (long long)L::Q * fm.nf;
     const S* lr = ODD ? f + QN : f;
     const S* lw = ODD ? f : f + QN;
     double sux = 0.0, srho = 0.0, ssp = 0.0, mx = 0.0, nonf = 0.0;
-    if (c < g.n) {
+    if (kk < fm.nf) {
+        // solid voxels of vel were zeroed before this launch
+        const int c = fm.cells[kk];
         float vx = 0.f, vy = 0.f, vz = 0.f;
-        const uint32_t nb = nbmask[c];
-        if (nb & kFluidBit) {
+        {
             typename Pop<S>::H h[L::Q];
-            gather<L, S>(lr, lw, c, nb, g, g.n, k.inv_scale, h);
+            gather<L, S>(lr, lw, kk, fm, g, k.inv_scale, h);
             const Moments<R, RA> m = moments<L, R, RA>(h, k.half_g);
             const RA ux = m.jx * m.inv_rho, uy = m.jy * m.inv_rho, uz = m.jz * m.inv_rho;
             vx = (float)ux;
@@ -434,45 +436,36 @@ __global__ void final_reduce_kernel(const double* __restrict__ partials, int nb,
     if (threadIdx.x < 5) out[threadIdx.x] = sh[threadIdx.x][0];
 }
 
-// Per-voxel neighbour mask: kFluidBit for a pore voxel, bit i (1..Q-1) when
-// the upstream voxel x - e_i (periodic) is rock.
-template <class L>
-__global__ void nbmask_kernel(const uint8_t* __restrict__ mat, Grid g, int pore,
-                              uint32_t* __restrict__ nbmask) {
+// Pore flags (set-up of the compacted layout).
+__global__ void fluid_flag_kernel(const uint8_t* __restrict__ mat, long long n, int pore,
+                                  uint8_t* __restrict__ flag) {
     const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= g.n) return;
-    const int z = (int)(c % g.nz);
-    const long long t = c / g.nz;
-    const int y = (int)(t % g.ny);
-    const int x = (int)(t / g.ny);
-    uint32_t m = (mat[c] == pore) ? kFluidBit : 0u;
-#pragma unroll
-    for (int i = 1; i < L::Q; ++i) {
-        int xx = x - L::c(i, 0), yy = y - L::c(i, 1), zz = z - L::c(i, 2);
-        xx = xx < 0 ? g.nx - 1 : (xx >= g.nx ? 0 : xx);
-        yy = yy < 0 ? g.ny - 1 : (yy >= g.ny ? 0 : yy);
-        zz = zz < 0 ? g.nz - 1 : (zz >= g.nz ? 0 : zz);
-        const long long s = ((long long)xx * g.ny + yy) * g.nz + zz;
-        if (mat[s] != pore) m |= 1u << i;
-    }
-    nbmask[c] = m;
+    if (c < n) flag[c] = (mat[c] == pore) ? 1 : 0;
+}
+
+// imap[cells[k]] = k (imap was filled with -1 first).
+__global__ void imap_scatter_kernel(const int* __restrict__ cells, int nf,
+                                    int* __restrict__ imap) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nf) imap[cells[k]] = k;
 }
 
 // -------------------------------------------------------------------------
 // launchers
 // -------------------------------------------------------------------------
-int flow_blocks(const Grid& g) { return (int)((g.n + kFlowThreads - 1) / kFlowThreads); }
+int flow_blocks(long long n) { return (int)((n + kFlowThreads - 1) / kFlowThreads); }
 
 template <class L, class M>
-static cudaError_t launch_step_t(bool odd, bool check, void* f, const uint32_t* nbm,
+static cudaError_t launch_step_t(bool odd, bool check, void* f, const FlowMap& fm,
                                  const Grid& g, const LbParams& k, const FlowCtrl* ctrl, int kstep,
                                  double* partials, cudaStream_t s) {
-    dim3 grid(flow_blocks(g));
+    if (fm.nf <= 0) return cudaSuccess;
+    dim3 grid(flow_blocks(fm.nf));
     typename M::S* fs = static_cast<typename M::S*>(f);
-    if (!odd && !check) lb_step_kernel<L, M, false, false><<<grid, kFlowThreads, 0, s>>>(fs, nbm, g, k, ctrl, kstep, partials);
-    if (!odd && check) lb_step_kernel<L, M, false, true><<<grid, kFlowThreads, 0, s>>>(fs, nbm, g, k, ctrl, kstep, partials);
-    if (odd && !check) lb_step_kernel<L, M, true, false><<<grid, kFlowThreads, 0, s>>>(fs, nbm, g, k, ctrl, kstep, partials);
-    if (odd && check) lb_step_kernel<L, M, true, true><<<grid, kFlowThreads, 0, s>>>(fs, nbm, g, k, ctrl, kstep, partials);
+    if (!odd && !check) lb_step_kernel<L, M, false, false><<<grid, kFlowThreads, 0, s>>>(fs, fm, g, k, ctrl, kstep, partials);
+    if (!odd && check) lb_step_kernel<L, M, false, true><<<grid, kFlowThreads, 0, s>>>(fs, fm, g, k, ctrl, kstep, partials);
+    if (odd && !check) lb_step_kernel<L, M, true, false><<<grid, kFlowThreads, 0, s>>>(fs, fm, g, k, ctrl, kstep, partials);
+    if (odd && check) lb_step_kernel<L, M, true, true><<<grid, kFlowThreads, 0, s>>>(fs, fm, g, k, ctrl, kstep, partials);
     return cudaGetLastError();
 }
 
@@ -489,9 +482,9 @@ static cudaError_t launch_step_t(bool odd, bool check, void* f, const uint32_t* 
     return FN<D2Q9, ModeF16>(__VA_ARGS__);
 
 cudaError_t flow_launch_step(int nd, int precision, bool odd, bool check, void* f,
-                             const uint32_t* nbm, const Grid& g, const LbParams& k,
+                             const FlowMap& fm, const Grid& g, const LbParams& k,
                              const FlowCtrl* ctrl, int kstep, double* partials, cudaStream_t s) {
-    PRT_DISPATCH(launch_step_t, odd, check, f, nbm, g, k, ctrl, kstep, partials, s)
+    PRT_DISPATCH(launch_step_t, odd, check, f, fm, g, k, ctrl, kstep, partials, s)
 }
 
 cudaError_t flow_launch_check(FlowCtrl* ctrl, const double* partials, int nblocks,
@@ -501,25 +494,30 @@ cudaError_t flow_launch_check(FlowCtrl* ctrl, const double* partials, int nblock
 }
 
 template <class L, class M>
-static cudaError_t launch_moments_t(bool odd, const void* f, const uint32_t* nbm, const Grid& g,
+static cudaError_t launch_moments_t(bool odd, const void* f, const FlowMap& fm, const Grid& g,
                                     const LbParams& k, float* vel, double* partials, cudaStream_t s) {
+    if (fm.nf <= 0) return cudaSuccess;
     const typename M::S* fs = static_cast<const typename M::S*>(f);
-    if (odd) lb_moments_kernel<L, M, true><<<flow_blocks(g), kFlowThreads, 0, s>>>(fs, nbm, g, k, vel, partials);
-    else lb_moments_kernel<L, M, false><<<flow_blocks(g), kFlowThreads, 0, s>>>(fs, nbm, g, k, vel, partials);
+    if (odd) lb_moments_kernel<L, M, true><<<flow_blocks(fm.nf), kFlowThreads, 0, s>>>(fs, fm, g, k, vel, partials);
+    else lb_moments_kernel<L, M, false><<<flow_blocks(fm.nf), kFlowThreads, 0, s>>>(fs, fm, g, k, vel, partials);
     return cudaGetLastError();
 }
 
 cudaError_t flow_launch_moments(int nd, int precision, bool odd, const void* f,
-                                const uint32_t* nbm, const Grid& g, const LbParams& k, float* vel,
+                                const FlowMap& fm, const Grid& g, const LbParams& k, float* vel,
                                 double* partials, cudaStream_t s) {
-    PRT_DISPATCH(launch_moments_t, odd, f, nbm, g, k, vel, partials, s)
+    PRT_DISPATCH(launch_moments_t, odd, f, fm, g, k, vel, partials, s)
 }
 
-cudaError_t flow_launch_nbmask(int nd, const uint8_t* mat, const Grid& g, int pore,
-                               uint32_t* nbmask, cudaStream_t s) {
-    const unsigned nb = (unsigned)((g.n + 255) / 256);
-    if (nd == 3) nbmask_kernel<D3Q19><<<nb, 256, 0, s>>>(mat, g, pore, nbmask);
-    else nbmask_kernel<D2Q9><<<nb, 256, 0, s>>>(mat, g, pore, nbmask);
+cudaError_t flow_launch_flags(const uint8_t* mat, long long n, int pore, uint8_t* flag,
+                              cudaStream_t s) {
+    fluid_flag_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(mat, n, pore, flag);
+    return cudaGetLastError();
+}
+
+cudaError_t flow_launch_imap(const int* cells, int nf, int* imap, cudaStream_t s) {
+    if (nf <= 0) return cudaSuccess;
+    imap_scatter_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(cells, nf, imap);
     return cudaGetLastError();
 }
 

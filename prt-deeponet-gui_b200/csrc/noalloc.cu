@@ -26,6 +26,7 @@
 //   - The solve runs on the calling thread's current device.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -68,15 +69,7 @@ cudaError_t scratch_addr(int dev, void** out) {
     return cudaSuccess;
 }
 
-__global__ void noalloc_count_kernel(const uint32_t* __restrict__ nbmask, long long n,
-                                     unsigned long long* out) {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int v = (c < n && (nbmask[c] & kFluidBit)) ? 1 : 0;
-    v = __syncthreads_count(v);
-    if (threadIdx.x == 0 && v) atomicAdd(out, (unsigned long long)v);
-}
-
-__global__ void noalloc_ctrl_kernel(FlowCtrl* ctrl, const unsigned long long* count, long long nit,
+__global__ void noalloc_ctrl_kernel(FlowCtrl* ctrl, const long long* count, long long nit,
                                     double tol, int every) {
     // control block of a fresh solve; the pore count comes from the device
     ctrl->it_base = 0;
@@ -124,16 +117,20 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
     if (g.n >= (1ll << 31)) return fail(PRT_E_INVALID, "grid too large");
     const int Q = p->nd == 3 ? 19 : 9;
     const size_t es = p->precision == PRT_FP64 ? 8 : (p->precision == PRT_FP16 ? 2 : 4);
-    const int nb = flow_blocks(g);
-    // scratch layout: control | count | 5 reduced sums | partials | masks | 2 lattices
+    // scratch layout, sized for the worst case (every voxel pore):
+    // control | count | 5 reduced sums | block counts | partials | flags |
+    // pore list | voxel -> slot map | 2 lattices
+    const int nb_max = flow_blocks(g.n);
     const size_t o_ctrl = 0;
     const size_t o_count = o_ctrl + up256(sizeof(FlowCtrl));
     const size_t o_out5 = o_count + 256;
-    const size_t o_part = o_out5 + 256;
-    const size_t o_mask = o_part + up256((size_t)nb * 5 * sizeof(double));
-    const size_t o_lat = o_mask + up256((size_t)g.n * 4);
-    const size_t lat_bytes = (size_t)2 * Q * g.n * es;
-    const size_t need = o_lat + lat_bytes;
+    const size_t o_cnt = o_out5 + 256;
+    const size_t o_part = o_cnt + up256((size_t)((g.n + 1023) / 1024) * 4);
+    const size_t o_flag = o_part + up256((size_t)nb_max * 5 * sizeof(double));
+    const size_t o_cells = o_flag + up256((size_t)g.n);
+    const size_t o_imap = o_cells + up256((size_t)g.n * 4);
+    const size_t o_lat = o_imap + up256((size_t)g.n * 4);
+    const size_t need = o_lat + (size_t)2 * Q * g.n * es;
     if (need > kNoAllocScratchBytes)
         return fail(PRT_E_INVALID,
                     "this grid needs " + std::to_string(need) + " bytes of scratch but the "
@@ -146,10 +143,13 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
     NCK(scratch_addr(dev, &base));
     unsigned char* sb = static_cast<unsigned char*>(base);
     FlowCtrl* ctrl = reinterpret_cast<FlowCtrl*>(sb + o_ctrl);
-    unsigned long long* count = reinterpret_cast<unsigned long long*>(sb + o_count);
+    long long* count = reinterpret_cast<long long*>(sb + o_count);
     double* out5 = reinterpret_cast<double*>(sb + o_out5);
+    int* cnt = reinterpret_cast<int*>(sb + o_cnt);
     double* parts = reinterpret_cast<double*>(sb + o_part);
-    uint32_t* nbmask = reinterpret_cast<uint32_t*>(sb + o_mask);
+    uint8_t* flag = sb + o_flag;
+    int* cells = reinterpret_cast<int*>(sb + o_cells);
+    int* imap = reinterpret_cast<int*>(sb + o_imap);
     void* f = sb + o_lat;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
@@ -186,11 +186,23 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
 
     // everything that must start at zero is cleared here: the array keeps
     // whatever the previous call left
-    NCK(cudaMemsetAsync(f, 0, lat_bytes, s));
-    NCK(cudaMemsetAsync(count, 0, sizeof(unsigned long long), s));
-    NCK(flow_launch_nbmask(p->nd, d_mat, g, 2, nbmask, s));
-    noalloc_count_kernel<<<(unsigned)((g.n + 255) / 256), 256, 0, s>>>(nbmask, g.n, count);
-    NCK(cudaGetLastError());
+    // pore-only layout: flags, count, pore list, voxel -> slot map
+    NCK(flow_launch_flags(d_mat, g.n, 2, flag, s));
+    NCK(adr_launch_compact(flag, g.n, cnt, count, nullptr, s));
+    long long nfluid = 0;
+    NCK(cudaMemcpyAsync(&nfluid, count, sizeof(nfluid), cudaMemcpyDeviceToHost, s));
+    NCK(cudaStreamSynchronize(s));
+    NCK(adr_launch_compact(flag, g.n, cnt, count, cells, s));
+    NCK(cudaMemsetAsync(imap, 0xff, (size_t)g.n * 4, s));
+    NCK(flow_launch_imap(cells, (int)nfluid, imap, s));
+    FlowMap fm;
+    fm.nf = (int)nfluid;
+    fm.cells = cells;
+    fm.imap = imap;
+    const int nb = std::max(flow_blocks(nfluid), 1);
+    NCK(cudaMemsetAsync(f, 0, (size_t)2 * Q * nfluid * es, s));
+    NCK(cudaMemsetAsync(d_vel_out, 0, (size_t)3 * g.n * sizeof(float), s));
+    NCK(cudaMemsetAsync(parts, 0, (size_t)nb * 5 * sizeof(double), s));
     noalloc_ctrl_kernel<<<1, 1, 0, s>>>(ctrl, count, p->nit, p->tol, p->every);
     NCK(cudaGetLastError());
 
@@ -205,7 +217,7 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
         for (int r = 0; r < 8 && launched < chunks; ++r, ++launched) {
             for (int kk = 0; kk < p->every; ++kk)
                 NCK(flow_launch_step(p->nd, p->precision, (kk & 1) != 0, kk == p->every - 1, f,
-                                     nbmask, g, k, ctrl, kk, parts, s));
+                                     fm, g, k, ctrl, kk, parts, s));
             NCK(flow_launch_check(ctrl, parts, nb, cudaGraphConditionalHandle(0), 0, s));
         }
         NCK(cudaMemcpyAsync(&hc, ctrl, sizeof(hc), cudaMemcpyDeviceToHost, s));
@@ -213,13 +225,11 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
     }
     NCK(cudaMemcpyAsync(&hc, ctrl, sizeof(hc), cudaMemcpyDeviceToHost, s));
     NCK(cudaStreamSynchronize(s));
-    NCK(flow_launch_moments(p->nd, p->precision, (hc.iters & 1) != 0, f, nbmask, g, k, d_vel_out,
+    NCK(flow_launch_moments(p->nd, p->precision, (hc.iters & 1) != 0, f, fm, g, k, d_vel_out,
                             parts, s));
     NCK(flow_launch_final_reduce(parts, nb, out5, s));
     double o5[5];
-    unsigned long long nfluid = 0;
     NCK(cudaMemcpyAsync(o5, out5, sizeof(o5), cudaMemcpyDeviceToHost, s));
-    NCK(cudaMemcpyAsync(&nfluid, count, sizeof(nfluid), cudaMemcpyDeviceToHost, s));
     NCK(cudaStreamSynchronize(s));
     if (info) {
         memset(info, 0, sizeof(*info));

@@ -101,24 +101,37 @@ struct PairTree {
     const int* level_off;  // nlevel + 1 offsets into the inner arrays
 };
 
+// The pore-only layout of a flow solve: lattice slot k holds pore voxel
+// cells[k] (C order); imap[voxel] is the slot of a pore voxel, -1 for rock.
+struct FlowMap {
+    int nf;
+    const int* cells;
+    const int* imap;
+};
+
 // Kernel launchers (lb_flow.cu) ---------------------------------------------
 // Returns cudaSuccess or the launch error.  f holds the two lattices (read /
-// write swap with the iteration parity), Q * n populations each.
-constexpr uint32_t kFluidBit = 1u << 31;  // in the per-voxel neighbour mask
+// write swap with the iteration parity), Q * nf populations each.  Step and
+// moments launches have flow_blocks(nf) blocks (the partial-sum count).
 cudaError_t flow_launch_step(int nd, int precision, bool odd, bool check, void* f,
-                             const uint32_t* nbmask, const Grid& g, const LbParams& lbp,
+                             const FlowMap& fm, const Grid& g, const LbParams& lbp,
                              const FlowCtrl* ctrl, int kstep, double* partials,
                              cudaStream_t s);
 cudaError_t flow_launch_check(FlowCtrl* ctrl, const double* partials, int nblocks,
                               cudaGraphConditionalHandle h, int use_handle, cudaStream_t s);
 cudaError_t flow_launch_moments(int nd, int precision, bool odd, const void* f,
-                                const uint32_t* nbmask, const Grid& g, const LbParams& lbp,
+                                const FlowMap& fm, const Grid& g, const LbParams& lbp,
                                 float* vel, double* partials, cudaStream_t s);
-cudaError_t flow_launch_nbmask(int nd, const uint8_t* mat, const Grid& g, int pore,
-                               uint32_t* nbmask, cudaStream_t s);
+cudaError_t flow_launch_flags(const uint8_t* mat, long long n, int pore, uint8_t* flag,
+                              cudaStream_t s);
+cudaError_t flow_launch_imap(const int* cells, int nf, int* imap, cudaStream_t s);
 cudaError_t flow_launch_final_reduce(const double* partials, int nblocks, double* out,
                                      cudaStream_t s);
-int flow_blocks(const Grid& g);
+int flow_blocks(long long n);
+// order-preserving compaction of a 0/1 flag array (adr.cu): with idx == NULL
+// only counts (cnt: one int per 1024 flags, *total on the device)
+cudaError_t adr_launch_compact(const uint8_t* mflag, long long n, int* cnt, long long* total,
+                               int* idx, cudaStream_t s);
 
 // Sets what prt_last_error(NULL) returns on the calling thread (runtime.cu).
 void set_noctx_error(const char* msg);

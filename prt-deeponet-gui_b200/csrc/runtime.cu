@@ -18,8 +18,6 @@
 using namespace prt;
 
 namespace prt {
-cudaError_t adr_launch_compact(const uint8_t* mflag, long long n, int* cnt, long long* total,
-                               int* idx, cudaStream_t s);
 cudaError_t adr_launch_chunk_means(const AdrDev& d, AdrCtrl* ctrl, const float** src_slot,
                                    float* means_out, cudaStream_t s);
 cudaError_t adr_launch_flags(const uint8_t* mat, const Grid& g, int nd, int pore, int bfc,
@@ -72,17 +70,18 @@ struct FlowKey {
     long long nit = -1;
     double tol = 0;
     void* f = nullptr;
-    void* aux[3] = {nullptr, nullptr, nullptr};
+    void* aux[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long nf = -1;  // pore voxels: launch sizes and the lattice stride are baked in
     bool operator==(const FlowKey& o) const {
         return nd == o.nd && precision == o.precision && every == o.every && g.nx == o.g.nx &&
                g.ny == o.g.ny && g.nz == o.g.nz && force == o.force && tau == o.tau &&
                magic == o.magic && nit == o.nit && tol == o.tol && f == o.f && aux[0] == o.aux[0] &&
-               aux[1] == o.aux[1] && aux[2] == o.aux[2];
+               aux[1] == o.aux[1] && aux[2] == o.aux[2] && aux[3] == o.aux[3] && nf == o.nf;
     }
 };
 
 struct FlowState {
-    DevBuf f, fluid, partials, ctrl, out5, count, mat, vel;
+    DevBuf f, fluid, partials, ctrl, out5, count, mat, vel, flag, cnt, cells;
     GraphHolder graph;
     FlowKey key;
 };
@@ -205,14 +204,6 @@ cudaError_t build_while_graph(cudaStream_t s, GraphHolder& gh, Emit emit) {
     return e;
 }
 
-__global__ void count_fluid_kernel(const uint32_t* __restrict__ nbmask, long long n,
-                                   unsigned long long* out) {
-    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int v = (c < n && (nbmask[c] & kFluidBit)) ? 1 : 0;
-    v = __syncthreads_count(v);
-    if (threadIdx.x == 0 && v) atomicAdd(out, (unsigned long long)v);
-}
-
 Grid make_grid(int nd, const int32_t* dims) {
     Grid g;
     if (nd == 3) {
@@ -302,7 +293,8 @@ extern "C" void prt_destroy(prt_ctx* c) {
     cudaStreamSynchronize(c->stream);
     c->adr.release();
     FlowState& f = c->flow;
-    DevBuf* all[] = {&f.f, &f.fluid, &f.partials, &f.ctrl, &f.out5, &f.count, &f.mat, &f.vel};
+    DevBuf* all[] = {&f.f,    &f.fluid, &f.partials, &f.ctrl, &f.out5, &f.count,
+                     &f.mat,  &f.vel,   &f.flag,     &f.cnt,  &f.cells};
     for (DevBuf* b : all) b->release();
     f.graph.release();
     for (int i = 0; i < 4; ++i)
@@ -367,27 +359,38 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
     const size_t es = p->precision == PRT_FP64 ? 8 : (p->precision == PRT_FP16 ? 2 : 4);
     if (g.n >= (1ll << 31))
         return fail(ctx, PRT_E_INVALID, "grids of 2^31 voxels or more are not supported");
-    const int nb = flow_blocks(g);
-    CK(F.f.ensure((size_t)2 * Q * g.n * es));  // two lattices
-    CK(F.fluid.ensure((size_t)g.n * 4));        // neighbour masks
+    // pore-only layout: flags, compacted voxel list, voxel -> slot map
+    CK(F.flag.ensure((size_t)g.n));
+    CK(F.cnt.ensure((size_t)((g.n + 1023) / 1024) * 4));
+    CK(F.count.ensure(sizeof(long long)));
+    CK(flow_launch_flags(d_mat, g.n, 2, F.flag.as<uint8_t>(), s));
+    CK(adr_launch_compact(F.flag.as<uint8_t>(), g.n, F.cnt.as<int>(), F.count.as<long long>(),
+                          nullptr, s));
+    long long nfluid = 0;
+    CK(cudaMemcpyAsync(&nfluid, F.count.p, sizeof(nfluid), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(F.cells.ensure((size_t)std::max(nfluid, 1ll) * 4));
+    CK(F.fluid.ensure((size_t)g.n * 4));  // imap
+    CK(adr_launch_compact(F.flag.as<uint8_t>(), g.n, F.cnt.as<int>(), F.count.as<long long>(),
+                          F.cells.as<int>(), s));
+    CK(cudaMemsetAsync(F.fluid.p, 0xff, (size_t)g.n * 4, s));
+    CK(flow_launch_imap(F.cells.as<int>(), (int)nfluid, F.fluid.as<int>(), s));
+    ctx->launches += 7;
+    FlowMap fm;
+    fm.nf = (int)nfluid;
+    fm.cells = F.cells.as<int>();
+    fm.imap = F.fluid.as<int>();
+    const int nb = std::max(flow_blocks(nfluid), 1);
+    CK(F.f.ensure((size_t)2 * Q * std::max(nfluid, 1ll) * es));  // two lattices
     CK(F.partials.ensure((size_t)nb * 5 * sizeof(double)));
     CK(F.ctrl.ensure(sizeof(FlowCtrl)));
     CK(F.out5.ensure(8 * sizeof(double)));
-    CK(F.count.ensure(sizeof(unsigned long long)));
 
-    // neighbour masks and the pore voxel count
-    CK(flow_launch_nbmask(p->nd, d_mat, g, 2, F.fluid.as<uint32_t>(), s));
-    CK(cudaMemsetAsync(F.count.p, 0, sizeof(unsigned long long), s));
-    count_fluid_kernel<<<(unsigned)((g.n + 255) / 256), 256, 0, s>>>(
-        F.fluid.as<uint32_t>(), g.n, F.count.as<unsigned long long>());
-    CK(cudaGetLastError());
-    ctx->launches += 2;
-    unsigned long long nfluid = 0;
-    CK(cudaMemcpyAsync(&nfluid, F.count.p, sizeof(nfluid), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-
-    // f = w_i everywhere, in both lattices: shifted storage h = 0
-    CK(cudaMemsetAsync(F.f.p, 0, (size_t)2 * Q * g.n * es, s));
+    // f = w_i everywhere, in both lattices: shifted storage h = 0; rock
+    // voxels of the output velocity are 0
+    CK(cudaMemsetAsync(F.f.p, 0, (size_t)2 * Q * nfluid * es, s));
+    CK(cudaMemsetAsync(d_vel, 0, (size_t)3 * g.n * sizeof(float), s));
+    CK(cudaMemsetAsync(F.partials.p, 0, (size_t)nb * 5 * sizeof(double), s));
     FlowCtrl hc{};
     hc.it_base = 0;
     hc.nit = p->nit;
@@ -414,7 +417,7 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
     auto emit = [&](cudaGraphConditionalHandle h, int use) -> cudaError_t {
         for (int k = 0; k < every; ++k) {
             cudaError_t e = flow_launch_step(p->nd, p->precision, (k & 1) != 0, k == every - 1,
-                                             F.f.p, F.fluid.as<uint32_t>(), g, kc, dctrl, k, parts, s);
+                                             F.f.p, fm, g, kc, dctrl, k, parts, s);
             if (e != cudaSuccess) return e;
         }
         return flow_launch_check(dctrl, parts, nb, h, use, s);
@@ -436,6 +439,7 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
             key.force = p->force; key.tau = p->tau; key.magic = p->magic; key.nit = p->nit;
             key.tol = p->tol; key.f = F.f.p;
             key.aux[0] = F.fluid.p; key.aux[1] = F.partials.p; key.aux[2] = F.ctrl.p;
+            key.aux[3] = F.cells.p; key.nf = nfluid;
             if (!F.graph.exec || !(key == F.key)) {
                 CK(build_while_graph(s, F.graph, emit));
                 F.key = key;
@@ -471,7 +475,7 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
         ctx->timing[1] = (double)res.iters;
     }
     // final field from the state after `iters` iterations
-    CK(flow_launch_moments(p->nd, p->precision, (res.iters & 1) != 0, F.f.p, F.fluid.as<uint32_t>(),
+    CK(flow_launch_moments(p->nd, p->precision, (res.iters & 1) != 0, F.f.p, fm,
                            g, kc, d_vel, parts, s));
     CK(flow_launch_final_reduce(parts, nb, F.out5.as<double>(), s));
     ctx->launches += 2;
