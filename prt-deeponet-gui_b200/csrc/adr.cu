@@ -9,251 +9,23 @@
 // is bit-identical to it, and so are the convergence means (numpy's float32
 // pairwise summation is replayed by adr_means_*), the stop step and the
 // snapshots.
-#include "prt_internal.h"
+#include "adr_core.cuh"
 
 namespace prt {
 
-// numpy's elementwise semantics ---------------------------------------------
-__device__ __forceinline__ float np_min(float a, float b) { return (a <= b || a != a) ? a : b; }
-__device__ __forceinline__ float np_max(float a, float b) { return (a >= b || a != a) ? a : b; }
-__device__ __forceinline__ float np_sign(float a) {
-    return a > 0.f ? 1.f : (a < 0.f ? -1.f : (a != a ? a : 0.f));
-}
-
-// _muscl (prtlb_3d.py:650-705): up + 1/2 minmod(down - up, up - upup), the
-// minmod written as 1/2 (sgn a + sgn b) min(|a|, |b|).
-__device__ __forceinline__ float muscl(float up, float upup, float down) {
-    const float d1 = down - up;
-    const float d2 = up - upup;
-    const float slope = (0.5f * (np_sign(d1) + np_sign(d2))) * np_min(fabsf(d1), fabsf(d2));
-    return up + 0.5f * slope;
-}
-
-template <int ND>
-struct Axes;
-template <>
-struct Axes<3> {
-    static constexpr int n = 3;
-    __host__ __device__ static constexpr int ax(int i) { return i; }
-};
-template <>
-struct Axes<2> {  // a 2D grid (nx, ny) is stored as (nx, 1, ny)
-    static constexpr int n = 2;
-    __host__ __device__ static constexpr int ax(int i) { return i == 0 ? 0 : 2; }
-};
-
-struct VoxelPos {
-    int p[3];
-    long long c;
-};
-
-__device__ __forceinline__ VoxelPos voxel_pos(long long c, const Grid& g) {
-    VoxelPos v;
-    v.c = c;
-    unsigned long long t = (unsigned long long)c;
-    v.p[2] = (int)(t % (unsigned)g.nz);
-    t /= (unsigned)g.nz;
-    v.p[1] = (int)(t % (unsigned)g.ny);
-    v.p[0] = (int)(t / (unsigned)g.ny);
-    return v;
-}
-
-__device__ __forceinline__ int extent(const Grid& g, int a) {
-    return a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
-}
-__device__ __forceinline__ long long stride(const Grid& g, int a) {
-    return a == 0 ? (long long)g.ny * g.nz : (a == 1 ? (long long)g.nz : 1ll);
-}
-// index of the low face of voxel v along axis a in the (n_a + 1)-long face array
-__device__ __forceinline__ long long face_lo(const Grid& g, const VoxelPos& v, int a) {
-    if (a == 0) return v.c;
-    if (a == 1) return ((long long)v.p[0] * (g.ny + 1) + v.p[1]) * g.nz + v.p[2];
-    return ((long long)v.p[0] * g.ny + v.p[1]) * (g.nz + 1) + v.p[2];
-}
-__device__ __forceinline__ long long face_step(const Grid& g, int a) {
-    return a == 0 ? (long long)g.ny * g.nz : (a == 1 ? (long long)g.nz : 1ll);
-}
-
-// A neighbour value of chemical j.  Every neighbour that is actually read is a
-// solute voxel (the open / far flags guarantee it), so it is on the inlet
-// plane exactly when its x is 0; there the pinned feed replaces the stored
-// value (step(), prtlb_3d.py:1392-1400, pins before transport).
-__device__ __forceinline__ float ld_c(const float* __restrict__ Cj, long long c, int x, bool pin,
-                                      float feed) {
-    return (pin && x == 0) ? feed : Cj[c];
-}
-
-// transport() of one chemical at one voxel (prtlb_3d.py:1182-1208).
-template <int ND>
-__device__ __forceinline__ float transport_one(const float* __restrict__ Cj, const Grid& g,
-                                               const VoxelPos& v, uint32_t fl,
-                                               const float* const* __restrict__ face, float Cc,
-                                               bool pin, float feed, const float (&dj)[3]) {
-    float out = 0.f;
-    float divu = 0.f;
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-        const int a = Axes<ND>::ax(i);
-        const int p = v.p[a];
-        const int n = extent(g, a);
-        const long long s = stride(g, a);
-        const bool oL = fl & f_open_lo(a), oH = fl & f_open_hi(a);
-        const bool fL = fl & f_far_lo(a), fH = fl & f_far_hi(a);
-        // clamped (edge-replicated) neighbour positions
-        const int pm1 = p > 0 ? p - 1 : 0, pm2 = p > 1 ? p - 2 : 0;
-        const int pp1 = p < n - 1 ? p + 1 : n - 1, pp2 = p < n - 2 ? p + 2 : n - 1;
-        const int x0 = v.p[0];
-        const int xm1 = (a == 0) ? pm1 : x0, xm2 = (a == 0) ? pm2 : x0;
-        const int xp1 = (a == 0) ? pp1 : x0, xp2 = (a == 0) ? pp2 : x0;
-        const float Cm1 = oL ? ld_c(Cj, v.c + (long long)(pm1 - p) * s, xm1, pin, feed) : Cc;
-        const float Cp1 = oH ? ld_c(Cj, v.c + (long long)(pp1 - p) * s, xp1, pin, feed) : Cc;
-        const float Cm2 = fL ? ld_c(Cj, v.c + (long long)(pm2 - p) * s, xm2, pin, feed) : Cm1;
-        const float Cp2 = fH ? ld_c(Cj, v.c + (long long)(pp2 - p) * s, xp2, pin, feed) : Cp1;
-        const long long fi = face_lo(g, v, a);
-        const float uL = face[a][fi];
-        const float uH = face[a][fi + face_step(g, a)];
-        const int bf = (fl & F_BF) ? 1 : 0;
-        // face diffusivity by the biofilm count of its two voxels (0, 1, 2);
-        // selected, not indexed, so the table stays in registers
-        const int nl = bf + ((fl & f_nbf_lo(a)) ? 1 : 0);
-        const int nh = bf + ((fl & f_nbf_hi(a)) ? 1 : 0);
-        const float DL = oL ? (nl == 0 ? dj[0] : (nl == 1 ? dj[1] : dj[2])) : 0.f;
-        const float DH = oH ? (nh == 0 ? dj[0] : (nh == 1 ? dj[1] : dj[2])) : 0.f;
-        // out += D_hi (C+1 - C) + D_lo (C-1 - C)
-        out = out + (DH * (Cp1 - Cc) + DL * (Cm1 - Cc));
-        const float fh = (uH >= 0.f) ? muscl(Cc, Cm1, Cp1) : muscl(Cp1, Cp2, Cc);
-        const float flo = (uL >= 0.f) ? muscl(Cm1, Cm2, Cc) : muscl(Cc, Cp1, Cm1);
-        // out -= u_hi f_hi - u_lo f_lo
-        out = out - (uH * fh - uL * flo);
-        divu = divu + (uH - uL);
-    }
-    return out + Cc * divu;
-}
-
-// The reaction terms (rate_biotic, rate_abiotic, reaction: prtlb_3d.py:1224-1367)
-// at one voxel, plus the reversible-sorption exchange (no reference counterpart).
-template <int NS>
-__device__ __forceinline__ void reaction(const float (&C)[NS], float surf,
-                                         const prt_adr_params& p, float (&dC)[NS]) {
-#pragma unroll
-    for (int j = 0; j < NS; ++j) dC[j] = 0.f;
-    float R = 0.f;
-    if (p.biotic_on) {
-        R = p.ks_donor_pos ? (p.k * C[0]) / (p.ks_donor + C[0]) : p.k * C[0];
-        if (NS > 1) R = R * (p.ks_acceptor_pos ? C[NS > 1 ? 1 : 0] / (p.ks_acceptor + C[NS > 1 ? 1 : 0])
-                                               : C[NS > 1 ? 1 : 0]);
-        if (NS > 3 && p.coupled) R = (R * C[NS > 3 ? 3 : 0]) / p.c3_init;
-        // caps: R <= 1/2 min(C0 / dt, C1 / (alpha dt))
-        float lim = C[0] / p.dt;
-        if (NS > 1 && p.alpha_cap) lim = np_min(lim, C[NS > 1 ? 1 : 0] / p.alpha_dt);
-        R = np_min(R, 0.5f * lim);
-    }
-    float Ra = 0.f;
-    if (p.abio_on) {
-        float cj = 0.f;
-#pragma unroll
-        for (int j = 0; j < NS; ++j)
-            if (j == p.j_ab) cj = C[j];
-        Ra = p.surface_only ? (p.ka * cj) * surf : p.ka * cj;
-        Ra = np_min(Ra, (0.5f * cj) / p.dt);
-    }
-    if (p.biotic_on) {
-        dC[0] = -R;
-        if (NS > 1) dC[NS > 1 ? 1 : 0] = p.neg_alpha * R;
-        if (NS > 2) dC[NS > 2 ? 2 : 0] = p.prod_coef * R;
-        if (NS > 3) dC[NS > 3 ? 3 : 0] = p.yield_ * R - p.kd * C[NS > 3 ? 3 : 0];
-    } else {
-        // R is the float32 scalar 0: -R, -alpha R, coef R are zeros, biomass 0
-    }
-    if (p.abio_on) {
-#pragma unroll
-        for (int j = 0; j < NS; ++j) {
-            if (j == p.j_ab) dC[j] = dC[j] - Ra;
-        }
-#pragma unroll
-        for (int j = 0; j < NS; ++j) {
-            if (j == p.j_mk && p.j_mk != p.j_ab) dC[j] = dC[j] + Ra;
-        }
-    }
-    if (p.sorp_on) {
-        float c = 0.f, s = 0.f;
-#pragma unroll
-        for (int j = 0; j < NS; ++j) {
-            if (j == p.j_c) c = C[j];
-            if (j == p.j_s) s = C[j];
-        }
-        float r = p.k_sorp * (c - s * p.inv_kd_sorp);
-        r = np_min(r, (0.5f * c) / p.dt);
-        r = np_max(r, -((0.5f * s) / p.dt));
-#pragma unroll
-        for (int j = 0; j < NS; ++j) {
-            if (j == p.j_c) dC[j] = dC[j] - r;
-            if (j == p.j_s) dC[j] = dC[j] + r;
-        }
-    }
-}
-
 constexpr int kAdrThreads = 256;
 
-// One transport step n = n_base + kstep + 1: reads the state after step n-1
-// from buf[(n-1)&1], writes the state after step n to buf[n&1] and, when n is
-// a snapshot step, also to its ladder slot.
+// One transport step n = n_base + kstep + 1 over every solute voxel (one
+// thread each; rock voxels are never touched and stay 0 in every buffer).
 template <int ND, int NS>
 __global__ void __launch_bounds__(kAdrThreads) adr_step_kernel(AdrDev d, prt_adr_params p,
                                                                const AdrCtrl* __restrict__ ctrl,
                                                                int kstep) {
     const long long n = ctrl->n_base + kstep + 1;
     if (ctrl->done || n > ctrl->limit) return;  // uniform over the grid
-    const long long c = (long long)blockIdx.x * kAdrThreads + threadIdx.x;
-    if (c >= d.g.n) return;
-    const uint32_t fl = d.flags[c];
-    if (!(fl & F_M)) return;  // rock: stays 0 in every buffer
-    const long long N = d.g.n;
-    const float* __restrict__ Cin = d.buf[(n - 1) & 1];
-    float* __restrict__ Cout = d.buf[n & 1];
-    const VoxelPos v = voxel_pos(c, d.g);
-    const bool x0 = fl & F_X0;
-    float C[NS];
-#pragma unroll
-    for (int j = 0; j < NS; ++j) {
-        const bool pin = (p.pinned_mask >> j) & 1u;
-        C[j] = (pin && x0) ? p.feed[j] : Cin[(long long)j * N + c];
-    }
-    float T[NS];
-#pragma unroll
-    for (int j = 0; j < NS; ++j) {
-        T[j] = 0.f;
-        if ((p.moving_mask >> j) & 1u) {
-            const bool pin = (p.pinned_mask >> j) & 1u;
-            const float dj[3] = {p.dface[j][0], p.dface[j][1], p.dface[j][2]};
-            T[j] = transport_one<ND>(Cin + (long long)j * N, d.g, v, fl, d.face, C[j], pin,
-                                     p.feed[j], dj);
-        }
-    }
-    float surf = 0.f;
-    if (p.abio_on && p.surface_only) {
-        float nface = 0.f;
-#pragma unroll
-        for (int i = 0; i < ND; ++i) {
-            const int a = Axes<ND>::ax(i);
-            nface = nface + ((fl & f_open_lo(a)) ? 0.f : 1.f);
-            nface = nface + ((fl & f_open_hi(a)) ? 0.f : 1.f);
-        }
-        surf = nface / (float)(2 * ND);
-    }
-    float dC[NS];
-    reaction<NS>(C, surf, p, dC);
-    const int slot = d.slot_of_step[n];
-    float* __restrict__ lad = slot >= 0 ? d.ladder + (long long)slot * NS * N : nullptr;
-#pragma unroll
-    for (int j = 0; j < NS; ++j) {
-        const bool mv = (p.moving_mask >> j) & 1u;
-        const float rhs = mv ? (T[j] + dC[j]) : dC[j];
-        float cn = C[j] + p.dt * rhs;
-        cn = np_max(cn, 0.f);
-        Cout[(long long)j * N + c] = cn;
-        if (lad) lad[(long long)j * N + c] = cn;
-    }
+    const long long kk = (long long)blockIdx.x * kAdrThreads + threadIdx.x;
+    if (kk >= d.nm) return;
+    adr_voxel<ND, NS>(d, p, n, kk);
 }
 
 // ---------------------------------------------------------------------------
@@ -388,7 +160,8 @@ __global__ void scatter_kernel(const uint8_t* __restrict__ mflag, long long n,
 }
 
 // ---------------------------------------------------------------------------
-// numpy float32 pairwise means (the stop rule's `C[j][m].mean()`)
+// numpy float32 pairwise means (the stop rule's `C[j][m].mean()`), per
+// species: leaf sums (leaf_sum) then the tree levels (tree_mean)
 // ---------------------------------------------------------------------------
 __global__ void means_leaf_kernel(const float* __restrict__ src, long long N,
                                   const int* __restrict__ idx, PairTree t, int ns,
@@ -397,51 +170,14 @@ __global__ void means_leaf_kernel(const float* __restrict__ src, long long N,
     if (tid >= (long long)t.nleaf * ns) return;
     const int leaf = (int)(tid % t.nleaf);
     const int j = (int)(tid / t.nleaf);
-    const float* s = src + (long long)j * N;
-    const int* ix = idx + t.leaf_start[leaf];
-    const int len = t.leaf_len[leaf];
-    float res;
-    if (len < 8) {
-        res = 0.f;
-        for (int i = 0; i < len; ++i) res = res + s[ix[i]];
-    } else {
-        float r0 = s[ix[0]], r1 = s[ix[1]], r2 = s[ix[2]], r3 = s[ix[3]];
-        float r4 = s[ix[4]], r5 = s[ix[5]], r6 = s[ix[6]], r7 = s[ix[7]];
-        int i = 8;
-        for (; i < len - (len % 8); i += 8) {
-            r0 = r0 + s[ix[i + 0]];
-            r1 = r1 + s[ix[i + 1]];
-            r2 = r2 + s[ix[i + 2]];
-            r3 = r3 + s[ix[i + 3]];
-            r4 = r4 + s[ix[i + 4]];
-            r5 = r5 + s[ix[i + 5]];
-            r6 = r6 + s[ix[i + 6]];
-            r7 = r7 + s[ix[i + 7]];
-        }
-        res = ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7));
-        for (; i < len; ++i) res = res + s[ix[i]];
-    }
-    vals[(long long)j * (t.nleaf + t.ninner) + leaf] = res;
+    vals[(long long)j * (t.nleaf + t.ninner) + leaf] = leaf_sum(src + (long long)j * N, idx, t, leaf);
 }
 
 __global__ void means_tree_kernel(PairTree t, long long nm, float* __restrict__ vals,
                                   float* __restrict__ means) {
     const int j = blockIdx.x;
-    float* v = vals + (long long)j * (t.nleaf + t.ninner);
-    for (int h = 0; h < t.nlevel; ++h) {
-        for (int i = t.level_off[h] + threadIdx.x; i < t.level_off[h + 1]; i += blockDim.x)
-            v[t.nleaf + i] = v[t.inner_l[i]] + v[t.inner_r[i]];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const float sum = t.root >= 0 ? 0.f + v[t.root] : 0.f;
-        means[j] = sum / (float)nm;  // 0/0 -> NaN for an empty pore space, as numpy
-    }
+    tree_mean(t, nm, vals + (long long)j * (t.nleaf + t.ninner), means + j);
 }
-
-// The check of the time loop (prtlb_3d.py:1499-1543), in float64 like the
-// reference's arrays of Python floats.
-__device__ __forceinline__ double npd_max(double a, double b) { return (a >= b || a != a) ? a : b; }
 
 __global__ void adr_stop_kernel(AdrCtrl* ctrl, const float* __restrict__ means, ProgressRec* log,
                                 int log_cap, cudaGraphConditionalHandle h, int use_handle) {
@@ -452,46 +188,7 @@ __global__ void adr_stop_kernel(AdrCtrl* ctrl, const float* __restrict__ means, 
     }
     const long long base = ctrl->n_base;
     const long long end = min(base + (long long)ctrl->check, ctrl->limit);
-    if (end > base && end % ctrl->check == 0) {
-        const int ns = ctrl->ns;
-        double cur[PRT_MAX_SPECIES], stepc[PRT_MAX_SPECIES];
-        double change = 0.0, rest = 0.0;
-        bool first = true;
-        for (int j = 0; j < ns; ++j) {
-            cur[j] = (double)means[j];
-            ctrl->scale[j] = npd_max(ctrl->scale[j], fabs(cur[j]));
-            stepc[j] = fabs(cur[j] - ctrl->prev[j]) / ctrl->scale[j];
-            const double r = ctrl->prev_change[j] > 0 ? stepc[j] / ctrl->prev_change[j] : 0.0;
-            double rj = (r < 1.0) ? stepc[j] * r / npd_max(1.0 - r, 1e-12) : INFINITY;
-            if (!isfinite(rj)) rj = INFINITY;
-            if (first) {
-                change = stepc[j];
-                rest = rj;
-                first = false;
-            } else {
-                change = (change != change) ? change : ((stepc[j] != stepc[j]) ? stepc[j] : fmax(change, stepc[j]));
-                rest = fmax(rest, rj);
-            }
-        }
-        if (ctrl->nlog < log_cap) {
-            ProgressRec& rec = log[ctrl->nlog];
-            rec.n = end;
-            rec.mean0 = cur[0];
-            rec.value = isfinite(rest) ? rest : change;
-        }
-        ctrl->nlog += 1;
-        ctrl->checks += 1;
-        ctrl->last_rest = rest;
-        if (ctrl->until_conv && end >= 10ll * ctrl->check && rest <= ctrl->tol) {
-            ctrl->converged = 1;
-            ctrl->done = 1;
-        } else {
-            for (int j = 0; j < ns; ++j) {
-                ctrl->prev[j] = cur[j];
-                ctrl->prev_change[j] = stepc[j];
-            }
-        }
-    }
+    if (end > base && end % ctrl->check == 0) adr_check(ctrl, means, end, log, log_cap);
     ctrl->n_base = end;
     if (end >= ctrl->limit) ctrl->done = 1;
     const int go = (!ctrl->done && end < ctrl->n_pause) ? 1 : 0;
@@ -513,36 +210,12 @@ __global__ void means_leaf_indirect_kernel(const AdrCtrl* __restrict__ ctrl, con
     const long long base = ctrl->n_base;
     const long long end = min(base + (long long)ctrl->check, ctrl->limit);
     if (!(end > base && end % ctrl->check == 0)) return;
-    const float* src = *src_p;
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (long long)t.nleaf * ns) return;
     const int leaf = (int)(tid % t.nleaf);
     const int j = (int)(tid / t.nleaf);
-    const float* s = src + (long long)j * N;
-    const int* ix = idx + t.leaf_start[leaf];
-    const int len = t.leaf_len[leaf];
-    float res;
-    if (len < 8) {
-        res = 0.f;
-        for (int i = 0; i < len; ++i) res = res + s[ix[i]];
-    } else {
-        float r0 = s[ix[0]], r1 = s[ix[1]], r2 = s[ix[2]], r3 = s[ix[3]];
-        float r4 = s[ix[4]], r5 = s[ix[5]], r6 = s[ix[6]], r7 = s[ix[7]];
-        int i = 8;
-        for (; i < len - (len % 8); i += 8) {
-            r0 = r0 + s[ix[i + 0]];
-            r1 = r1 + s[ix[i + 1]];
-            r2 = r2 + s[ix[i + 2]];
-            r3 = r3 + s[ix[i + 3]];
-            r4 = r4 + s[ix[i + 4]];
-            r5 = r5 + s[ix[i + 5]];
-            r6 = r6 + s[ix[i + 6]];
-            r7 = r7 + s[ix[i + 7]];
-        }
-        res = ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7));
-        for (; i < len; ++i) res = res + s[ix[i]];
-    }
-    vals[(long long)j * (t.nleaf + t.ninner) + leaf] = res;
+    vals[(long long)j * (t.nleaf + t.ninner) + leaf] =
+        leaf_sum(*src_p + (long long)j * N, idx, t, leaf);
 }
 
 __global__ void means_tree_cond_kernel(const AdrCtrl* __restrict__ ctrl, PairTree t, long long nm,
@@ -552,16 +225,7 @@ __global__ void means_tree_cond_kernel(const AdrCtrl* __restrict__ ctrl, PairTre
     const long long end = min(base + (long long)ctrl->check, ctrl->limit);
     if (!(end > base && end % ctrl->check == 0)) return;
     const int j = blockIdx.x;
-    float* v = vals + (long long)j * (t.nleaf + t.ninner);
-    for (int h = 0; h < t.nlevel; ++h) {
-        for (int i = t.level_off[h] + threadIdx.x; i < t.level_off[h + 1]; i += blockDim.x)
-            v[t.nleaf + i] = v[t.inner_l[i]] + v[t.inner_r[i]];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const float sum = t.root >= 0 ? 0.f + v[t.root] : 0.f;
-        means[j] = sum / (float)nm;
-    }
+    tree_mean(t, nm, vals + (long long)j * (t.nleaf + t.ninner), means + j);
 }
 
 // ---------------------------------------------------------------------------
@@ -570,7 +234,8 @@ __global__ void means_tree_cond_kernel(const AdrCtrl* __restrict__ ctrl, PairTre
 template <int ND, int NS>
 static cudaError_t step_t(const AdrDev& d, const prt_adr_params& p, AdrCtrl* ctrl, int k,
                           cudaStream_t s) {
-    const unsigned nb = (unsigned)((d.g.n + kAdrThreads - 1) / kAdrThreads);
+    if (d.nm <= 0) return cudaSuccess;
+    const unsigned nb = (unsigned)((d.nm + kAdrThreads - 1) / kAdrThreads);
     adr_step_kernel<ND, NS><<<nb, kAdrThreads, 0, s>>>(d, p, ctrl, k);
     return cudaGetLastError();
 }

@@ -21,232 +21,9 @@
 // Populations are stored shifted, h_i = f_i - w_i: the non-equilibrium part
 // that carries the viscous stress is of the order of the force (1e-7) and
 // would drown next to w_i ~ 0.3 in float32 (prtlb_2d.py:354-362).
-#include <cuda_fp16.h>
-
-#include "prt_internal.h"
+#include "lb_core.cuh"
 
 namespace prt {
-
-// -------------------------------------------------------------------------
-// Lattices, in the storage frame (x, y, z).  The direction order and weights
-// are the reference's (prtlb_3d.py:370-375, prtlb_2d.py:391-394); a D2Q9
-// direction (ex, ey) is stored as (ex, 0, ey) because 2D grids are kept as
-// (nx, 1, ny).
-// -------------------------------------------------------------------------
-struct D3Q19 {
-    static constexpr int Q = 19;
-    static constexpr int NP = 9;
-    __host__ __device__ static constexpr int c(int i, int a) {
-        return (a == 0) ? (i == 1 || i == 7 || i == 9 || i == 11 || i == 13   ? 1
-                           : i == 2 || i == 8 || i == 10 || i == 12 || i == 14 ? -1
-                                                                                : 0)
-             : (a == 1) ? (i == 3 || i == 7 || i == 10 || i == 15 || i == 17   ? 1
-                           : i == 4 || i == 8 || i == 9 || i == 16 || i == 18  ? -1
-                                                                                : 0)
-                        : (i == 5 || i == 11 || i == 14 || i == 15 || i == 18  ? 1
-                           : i == 6 || i == 12 || i == 13 || i == 16 || i == 17 ? -1
-                                                                                 : 0);
-    }
-    // pairs (a, b) with e_b = -e_a
-    __host__ __device__ static constexpr int pa(int p) { return 2 * p + 1; }
-    __host__ __device__ static constexpr int pb(int p) { return 2 * p + 2; }
-    __host__ __device__ static constexpr int opp(int i) {
-        return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1);
-    }
-    __host__ __device__ static constexpr double w(int i) {
-        return i == 0 ? 1.0 / 3.0 : (i < 7 ? 1.0 / 18.0 : 1.0 / 36.0);
-    }
-};
-
-struct D2Q9 {
-    static constexpr int Q = 9;
-    static constexpr int NP = 4;
-    // reference order: (0,0) (1,0) (0,1) (-1,0) (0,-1) (1,1) (-1,1) (-1,-1) (1,-1)
-    __host__ __device__ static constexpr int ex(int i) {
-        return (i == 1 || i == 5 || i == 8) ? 1 : ((i == 3 || i == 6 || i == 7) ? -1 : 0);
-    }
-    __host__ __device__ static constexpr int ey(int i) {
-        return (i == 2 || i == 5 || i == 6) ? 1 : ((i == 4 || i == 7 || i == 8) ? -1 : 0);
-    }
-    __host__ __device__ static constexpr int c(int i, int a) {
-        return a == 0 ? ex(i) : (a == 1 ? 0 : ey(i));
-    }
-    __host__ __device__ static constexpr int pa(int p) { return p < 2 ? p + 1 : p + 3; }
-    __host__ __device__ static constexpr int pb(int p) { return p < 2 ? p + 3 : p + 5; }
-    __host__ __device__ static constexpr int opp(int i) {
-        return i == 0 ? 0 : (i < 5 ? ((i + 1) % 4) + 1 : ((i - 3) % 4) + 5);
-    }
-    __host__ __device__ static constexpr double w(int i) {
-        return i == 0 ? 4.0 / 9.0 : (i < 5 ? 1.0 / 9.0 : 1.0 / 36.0);
-    }
-};
-
-// storage conversions ------------------------------------------------------
-// Pop<S>::H is the register type a stored population is held in; st() rounds
-// the collision result to the storage type once.
-template <class S>
-struct Pop;
-template <>
-struct Pop<double> {
-    using H = double;
-    __device__ static double ld(const double* p, float) { return *p; }
-    template <class R>
-    __device__ static void st(double* p, R v, float) { *p = (double)v; }
-};
-template <>
-struct Pop<float> {
-    using H = float;
-    __device__ static float ld(const float* p, float) { return *p; }
-    template <class R>
-    __device__ static void st(float* p, R v, float) { *p = (float)v; }
-};
-template <>
-struct Pop<__half> {
-    using H = float;
-    __device__ static float ld(const __half* p, float inv) { return __half2float(*p) * inv; }
-    template <class R>
-    __device__ static void st(__half* p, R v, float scale) {
-        float s = (float)v * scale;
-        s = fminf(fmaxf(s, -65504.f), 65504.f);
-        *p = __float2half_rn(s);
-    }
-};
-
-// Precision modes: storage type S, arithmetic R for the symmetric part and
-// RA for the momentum and the antisymmetric non-equilibrium part (a small
-// difference of two O(u) numbers), and the resident 256-thread blocks per SM
-// the register budget is cut for.
-struct ModeF64 {  // the reference's arithmetic
-    using S = double;
-    using R = double;
-    using RA = double;
-    static constexpr int min_blocks = 2;
-};
-struct ModeF32 {  // float32 populations, float32 collision
-    using S = float;
-    using R = float;
-    using RA = float;
-    static constexpr int min_blocks = 3;
-};
-struct ModeF32D {  // float32 populations, float64 momentum
-    using S = float;
-    using R = float;
-    using RA = double;
-    static constexpr int min_blocks = 3;
-};
-struct ModeF16 {  // scaled float16 populations, float32 collision
-    using S = __half;
-    using R = float;
-    using RA = float;
-    static constexpr int min_blocks = 3;
-};
-
-// Gather the arrived populations of pore voxel number k (see the file
-// comment).  Lattices hold the pore voxels only, in C order: voxel
-// cells[k] is slot k, and imap[voxel] is the slot of a pore voxel or -1.
-template <class L, class S>
-__device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __restrict__ lw, int k,
-                                       const FlowMap& fm, const Grid& g, float inv,
-                                       typename Pop<S>::H (&h)[L::Q]) {
-    const long long NF = fm.nf;
-    const int v = fm.cells[k];
-    const int z = v % g.nz;
-    const int t = v / g.nz;
-    const int y = t % g.ny;
-    const int x = t / g.ny;
-    const int syz = g.ny * g.nz;
-    int src[L::Q];
-#pragma unroll
-    for (int i = 1; i < L::Q; ++i) {
-        const int dx = -L::c(i, 0), dy = -L::c(i, 1), dz = -L::c(i, 2);
-        int xx = x + dx, yy = y + dy, zz = z + dz;
-        if (dx) xx = xx < 0 ? g.nx - 1 : (xx >= g.nx ? 0 : xx);
-        if (dy) yy = yy < 0 ? g.ny - 1 : (yy >= g.ny ? 0 : yy);
-        if (dz) zz = zz < 0 ? g.nz - 1 : (zz >= g.nz ? 0 : zz);
-        src[i] = fm.imap[xx * syz + yy * g.nz + zz];
-    }
-    h[0] = Pop<S>::ld(lr + k, inv);
-#pragma unroll
-    for (int i = 1; i < L::Q; ++i) {
-        h[i] = src[i] >= 0 ? Pop<S>::ld(lr + (long long)i * NF + src[i], inv)
-                           : Pop<S>::ld(lw + (long long)L::opp(i) * NF + k, inv);
-    }
-}
-
-template <class R, class RA>
-struct Moments {
-    R drho, jsq;    // density deviation, rho u^2
-    RA jx, jy, jz;  // J = rho u (with the half force on x)
-    RA inv_rho;
-};
-
-// Moments of the arrived (shifted) populations (prtlb_3d.py:428-433):
-// drho = sum h, J = rho u = sum e h + g/2 x.
-template <class L, class R, class RA, class H>
-__device__ __forceinline__ Moments<R, RA> moments(const H (&h)[L::Q], double half_g) {
-    Moments<R, RA> m;
-    RA s = RA(h[0]);
-    RA jx = RA(0), jy = RA(0), jz = RA(0);
-#pragma unroll
-    for (int p = 0; p < L::NP; ++p) {
-        const int a = L::pa(p), b = L::pb(p);
-        s += RA(h[a]) + RA(h[b]);
-        const RA d = RA(h[a]) - RA(h[b]);
-        if (L::c(a, 0) == 1) jx += d;
-        if (L::c(a, 0) == -1) jx -= d;
-        if (L::c(a, 1) == 1) jy += d;
-        if (L::c(a, 1) == -1) jy -= d;
-        if (L::c(a, 2) == 1) jz += d;
-        if (L::c(a, 2) == -1) jz -= d;
-    }
-    jx += RA(half_g);
-    m.jx = jx;
-    m.jy = jy;
-    m.jz = jz;
-    const RA rho = RA(1) + s;
-    m.inv_rho = RA(1) / rho;
-    m.drho = R(s);
-    m.jsq = R((jx * jx + jy * jy + jz * jz) * m.inv_rho);  // rho u^2 = |J|^2 / rho
-    return m;
-}
-
-// TRT collision (_trt_collide, prtlb_3d.py:142-154) + Guo forcing in the
-// shifted variables, written with J = rho u so that rho cancels in the
-// antisymmetric equilibrium (w rho 3 e.u = 3 w e.J) and rho u u = J J / rho in
-// the symmetric one.  The new population is h + delta with delta summed
-// first, so the stored result rounds once; it goes to slot i of voxel c.
-template <class L, class S, class R, class RA>
-__device__ __forceinline__ void collide_store(S* __restrict__ lw, int c, long long N,
-                                              const typename Pop<S>::H (&h)[L::Q],
-                                              const Moments<R, RA>& m, const LbParams& kc) {
-    const R omp = R(kc.omp);
-    const R inv_rho = R(m.inv_rho);
-    const R heq0 = R(L::w(0)) * (m.drho - R(1.5) * m.jsq);
-    const R h0 = R(h[0]);
-    Pop<S>::st(lw + c, h0 - omp * (h0 - heq0), kc.scale);
-#pragma unroll
-    for (int p = 0; p < L::NP; ++p) {
-        const int a = L::pa(p), b = L::pb(p);
-        RA eJ = RA(0);
-        if (L::c(a, 0) == 1) eJ += m.jx;
-        if (L::c(a, 0) == -1) eJ -= m.jx;
-        if (L::c(a, 1) == 1) eJ += m.jy;
-        if (L::c(a, 1) == -1) eJ -= m.jy;
-        if (L::c(a, 2) == 1) eJ += m.jz;
-        if (L::c(a, 2) == -1) eJ -= m.jz;
-        const R eJr = R(eJ);
-        const R heq_p = R(L::w(a)) * (m.drho + (R(4.5) * eJr * eJr * inv_rho - R(1.5) * m.jsq));
-        const R ha = R(h[a]), hb = R(h[b]);
-        const R dp = omp * (R(0.5) * (ha + hb) - heq_p);
-        const RA dma = RA(kc.omm) * (RA(0.5) * (RA(h[a]) - RA(h[b])) - RA(3.0 * L::w(a)) * eJ);
-        const R dm = R(dma);
-        const R gp = R(kc.guo[p]);
-        Pop<S>::st(lw + (long long)a * N + c, ha + ((gp - dp) - dm), kc.scale);
-        Pop<S>::st(lw + (long long)b * N + c, hb + ((dm - dp) - gp), kc.scale);
-    }
-}
-
-constexpr int kFlowThreads = 256;
 
 // One whole LB iteration t: lattice (t & 1) is read, lattice ((t + 1) & 1)
 // written; solid voxels do nothing.
@@ -254,22 +31,13 @@ template <class L, class M, bool ODD, bool CHECK>
 __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
     lb_step_kernel(typename M::S* __restrict__ f, FlowMap fm, Grid g, LbParams kc,
                    const FlowCtrl* __restrict__ ctrl, int kstep, double* __restrict__ partials) {
-    using S = typename M::S;
-    using R = typename M::R;
-    using RA = typename M::RA;
     const long long it = ctrl->it_base + kstep;
     if (ctrl->done || it >= ctrl->nit) return;  // uniform over the grid
     const int k = blockIdx.x * kFlowThreads + threadIdx.x;
-    const long long QN = (long long)L::Q * fm.nf;
-    const S* lr = ODD ? f + QN : f;
-    S* lw = ODD ? f : f + QN;
     double acc = 0.0;
     if (k < fm.nf) {
-        typename Pop<S>::H h[L::Q];
-        gather<L, S>(lr, lw, k, fm, g, kc.inv_scale, h);
-        const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
-        collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
-        if (CHECK) acc = fabs((double)m.jx * (double)m.inv_rho);
+        const double ux = lb_cell<L, M, ODD>(f, fm, g, kc, k);
+        if (CHECK) acc = ux;
     }
     if (CHECK) {
         __shared__ double sh[kFlowThreads / 32];

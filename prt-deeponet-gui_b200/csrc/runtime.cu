@@ -84,6 +84,15 @@ struct FlowState {
     DevBuf f, fluid, partials, ctrl, out5, count, mat, vel, flag, cnt, cells;
     GraphHolder graph;
     FlowKey key;
+    // the solve set up by flow_setup
+    prt_flow_params p{};
+    Grid g{0, 0, 0, 0};
+    FlowMap fm{0, nullptr, nullptr};
+    LbParams kc{};
+    int nb = 1;
+    long long nfluid = 0;
+    float scale = 1.f;
+    float* d_vel = nullptr;
 };
 
 struct AdrState {
@@ -99,6 +108,8 @@ struct AdrState {
     const uint8_t* d_mat = nullptr;  // staged inputs (borrowed until begin)
     const float* d_vel = nullptr;
     DevBuf tmp, vstats;
+    std::vector<long long> sched;       // ladder step schedule of the run
+    prt_adr_run_params rp{};
     std::vector<long long> keep_steps;  // ladder step numbers
     std::vector<int> slot_of_index;     // ladder index -> slot
     int nslots = 0;
@@ -336,8 +347,10 @@ extern "C" size_t prt_sizeof(int which) {
 // ===========================================================================
 // flow
 // ===========================================================================
-extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p,
-                            float* d_vel, prt_flow_info* info) {
+// Flow solve in three parts, so the batched engine can run many set-up
+// solves through one time loop: set-up (buffers, pore-only layout, control
+// block, constants), the time loop, and the final field with its reductions.
+int flow_setup(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p, float* d_vel) {
     if (!ctx || !p || !d_mat || !d_vel) return fail(ctx, PRT_E_INVALID, "null argument");
     if (p->nd != 2 && p->nd != 3) return fail(ctx, PRT_E_INVALID, "nd must be 2 or 3");
     for (int i = 0; i < p->nd; ++i)
@@ -376,13 +389,12 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
     CK(cudaMemsetAsync(F.fluid.p, 0xff, (size_t)g.n * 4, s));
     CK(flow_launch_imap(F.cells.as<int>(), (int)nfluid, F.fluid.as<int>(), s));
     ctx->launches += 7;
-    FlowMap fm;
-    fm.nf = (int)nfluid;
-    fm.cells = F.cells.as<int>();
-    fm.imap = F.fluid.as<int>();
-    const int nb = std::max(flow_blocks(nfluid), 1);
+    F.fm.nf = (int)nfluid;
+    F.fm.cells = F.cells.as<int>();
+    F.fm.imap = F.fluid.as<int>();
+    F.nb = std::max(flow_blocks(nfluid), 1);
     CK(F.f.ensure((size_t)2 * Q * std::max(nfluid, 1ll) * es));  // two lattices
-    CK(F.partials.ensure((size_t)nb * 5 * sizeof(double)));
+    CK(F.partials.ensure((size_t)F.nb * 5 * sizeof(double)));
     CK(F.ctrl.ensure(sizeof(FlowCtrl)));
     CK(F.out5.ensure(8 * sizeof(double)));
 
@@ -390,7 +402,7 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
     // voxels of the output velocity are 0
     CK(cudaMemsetAsync(F.f.p, 0, (size_t)2 * Q * nfluid * es, s));
     CK(cudaMemsetAsync(d_vel, 0, (size_t)3 * g.n * sizeof(float), s));
-    CK(cudaMemsetAsync(F.partials.p, 0, (size_t)nb * 5 * sizeof(double), s));
+    CK(cudaMemsetAsync(F.partials.p, 0, (size_t)F.nb * 5 * sizeof(double), s));
     FlowCtrl hc{};
     hc.it_base = 0;
     hc.nit = p->nit;
@@ -402,15 +414,63 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
     hc.every = p->every;
     hc.done = p->nit == 0 ? 1 : 0;
     CK(cudaMemcpyAsync(F.ctrl.p, &hc, sizeof(hc), cudaMemcpyHostToDevice, s));
-
-    float scale = 1.f;
+    F.scale = 1.f;
     if (p->precision == PRT_FP16) {
         const double g0 = std::fabs(p->force) > 0 ? std::fabs(p->force) : 1e-6;
-        scale = (float)std::ldexp(1.0, (int)std::floor(std::log2(1.0 / g0)));
+        F.scale = (float)std::ldexp(1.0, (int)std::floor(std::log2(1.0 / g0)));
     }
-    LbParams kc;
-    fill_lbconst(kc, p->nd, p->force, p->tau, p->magic, scale);
+    fill_lbconst(F.kc, p->nd, p->force, p->tau, p->magic, F.scale);
+    F.p = *p;
+    F.g = g;
+    F.nfluid = nfluid;
+    F.d_vel = d_vel;
+    return PRT_OK;
+}
 
+int flow_finish(prt_ctx* ctx, prt_flow_info* info) {
+    FlowState& F = ctx->flow;
+    cudaStream_t s = ctx->stream;
+    FlowCtrl res;
+    CK(cudaMemcpyAsync(&res, F.ctrl.p, sizeof(res), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    // final field from the state after `iters` iterations
+    double* parts = F.partials.as<double>();
+    CK(flow_launch_moments(F.p.nd, F.p.precision, (res.iters & 1) != 0, F.f.p, F.fm, F.g, F.kc,
+                           F.d_vel, parts, s));
+    CK(flow_launch_final_reduce(parts, F.nb, F.out5.as<double>(), s));
+    ctx->launches += 2;
+    double o5[5];
+    CK(cudaMemcpyAsync(o5, F.out5.p, sizeof(o5), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (info) {
+        memset(info, 0, sizeof(*info));
+        info->iters = res.iters;
+        info->converged = res.converged;
+        info->change = res.change;
+        info->fluid_cells = (int64_t)F.nfluid;
+        info->ux_sum = o5[0];
+        info->mass = o5[1];
+        info->speed_sum = o5[2];
+        info->umax = o5[3];
+        info->nonfinite = (int64_t)llround(o5[4]);
+        const double nu = (F.p.tau - 0.5) / 3.0;
+        info->permeability =
+            F.p.force != 0 ? nu * (o5[0] / (double)F.g.n) / F.p.force : 0.0;
+        info->fp16_scale = F.scale;
+    }
+    return PRT_OK;
+}
+
+extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p,
+                            float* d_vel, prt_flow_info* info) {
+    int rc = flow_setup(ctx, d_mat, p, d_vel);
+    if (rc != PRT_OK) return rc;
+    FlowState& F = ctx->flow;
+    cudaStream_t s = ctx->stream;
+    const Grid g = F.g;
+    const FlowMap fm = F.fm;
+    const LbParams kc = F.kc;
+    const int nb = F.nb;
     FlowCtrl* dctrl = F.ctrl.as<FlowCtrl>();
     double* parts = F.partials.as<double>();
     const int every = p->every;
@@ -423,10 +483,10 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
         return flow_launch_check(dctrl, parts, nb, h, use, s);
     };
     CK(cudaEventRecord(ctx->ev[0], s));
-    if (hc.done == 0) {
+    if (p->nit > 0) {
         if (graphs_disabled()) {
             // direct launches, chunk by chunk
-            FlowCtrl hc2 = hc;
+            FlowCtrl hc2{};
             while (!hc2.done) {
                 CK(emit(cudaGraphConditionalHandle(0), 0));
                 ctx->launches += every + 1;
@@ -439,7 +499,7 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
             key.force = p->force; key.tau = p->tau; key.magic = p->magic; key.nit = p->nit;
             key.tol = p->tol; key.f = F.f.p;
             key.aux[0] = F.fluid.p; key.aux[1] = F.partials.p; key.aux[2] = F.ctrl.p;
-            key.aux[3] = F.cells.p; key.nf = nfluid;
+            key.aux[3] = F.cells.p; key.nf = F.nfluid;
             if (!F.graph.exec || !(key == F.key)) {
                 CK(build_while_graph(s, F.graph, emit));
                 F.key = key;
@@ -452,7 +512,7 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
                 CK(cudaStreamSynchronize(s));
                 ctx->launches += (hc2.iters + every - 1) / every * (every + 1);
             } else {
-                FlowCtrl hc2 = hc;
+                FlowCtrl hc2{};
                 long long launched = 0;
                 while (!hc2.done && launched < chunks) {
                     for (int r = 0; r < 20 && launched < chunks; ++r, ++launched)
@@ -465,39 +525,17 @@ extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_p
         }
     }
     CK(cudaEventRecord(ctx->ev[1], s));
-    FlowCtrl res;
-    CK(cudaMemcpyAsync(&res, dctrl, sizeof(res), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    CK(cudaEventSynchronize(ctx->ev[1]));
     {
+        FlowCtrl res;
+        CK(cudaMemcpyAsync(&res, dctrl, sizeof(res), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
         ctx->timing[0] = ms;
         ctx->timing[1] = (double)res.iters;
     }
-    // final field from the state after `iters` iterations
-    CK(flow_launch_moments(p->nd, p->precision, (res.iters & 1) != 0, F.f.p, fm,
-                           g, kc, d_vel, parts, s));
-    CK(flow_launch_final_reduce(parts, nb, F.out5.as<double>(), s));
-    ctx->launches += 2;
-    double o5[5];
-    CK(cudaMemcpyAsync(o5, F.out5.p, sizeof(o5), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    if (info) {
-        memset(info, 0, sizeof(*info));
-        info->iters = res.iters;
-        info->converged = res.converged;
-        info->change = res.change;
-        info->fluid_cells = (int64_t)nfluid;
-        info->ux_sum = o5[0];
-        info->mass = o5[1];
-        info->speed_sum = o5[2];
-        info->umax = o5[3];
-        info->nonfinite = (int64_t)llround(o5[4]);
-        const double nu = (p->tau - 0.5) / 3.0;
-        info->permeability = p->force != 0 ? nu * (o5[0] / (double)g.n) / p->force : 0.0;
-        info->fp16_scale = scale;
-    }
-    return PRT_OK;
+    return flow_finish(ctx, info);
 }
 
 extern "C" int prt_flow(prt_ctx* ctx, const uint8_t* mat, const prt_flow_params* p, float* vel_out,
@@ -723,8 +761,9 @@ extern "C" int prt_adr_begin(prt_ctx* ctx, const prt_adr_params* p) {
     return PRT_OK;
 }
 
-extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progress_cb cb,
-                           void* user, prt_adr_result* res) {
+// Transport time loop in three parts (see flow_setup): the ladder and the
+// control block, the loop, and the kept snapshots.
+int adr_run_setup(prt_ctx* ctx, const prt_adr_run_params* rp, long long pause_every) {
     if (!ctx || !rp) return fail(ctx, PRT_E_INVALID, "null argument");
     AdrState& A = ctx->adr;
     if (!A.begun) return fail(ctx, PRT_E_STATE, "prt_adr_run before prt_adr_begin");
@@ -737,24 +776,24 @@ extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progr
     const long long limit = rp->limit;
     // the snapshot ladder (prtlb_3d.py:1496-1498): record at n >= nxt,
     // nxt = max(n + 1, ceil(n * ratio)); steps are known before the run
-    std::vector<long long> sched;
+    A.sched.clear();
     {
         long long nxt = 1;
         for (long long n = nxt; n <= limit;) {
-            sched.push_back(n);
+            A.sched.push_back(n);
             long long c2 = (long long)std::ceil((double)n * rp->ratio);
             nxt = std::max(n + 1, c2);
             n = nxt;
         }
     }
-    const int K = (int)sched.size();
+    const int K = (int)A.sched.size();
     A.nslots = K + 2;  // step 0, the schedule, and a final record
     const size_t slot_bytes = (size_t)N * ns * 4;
     CK(A.ladder.ensure(slot_bytes * A.nslots));
     CK(cudaMemsetAsync(A.ladder.p, 0, slot_bytes * A.nslots, s));
     CK(cudaMemcpyAsync(A.ladder.p, A.buf[0].p, slot_bytes, cudaMemcpyDeviceToDevice, s));
     std::vector<int> sos((size_t)limit + 1, -1);
-    for (int k = 0; k < K; ++k) sos[(size_t)sched[k]] = k + 1;
+    for (int k = 0; k < K; ++k) sos[(size_t)A.sched[k]] = k + 1;
     CK(A.slot_of_step.ensure(sos.size() * 4));
     CK(cudaMemcpyAsync(A.slot_of_step.p, sos.data(), sos.size() * 4, cudaMemcpyHostToDevice, s));
     const int log_cap = (int)(limit / rp->check) + 2;
@@ -777,13 +816,63 @@ extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progr
         hc.prev_change[j] = 0.0;
         hc.scale[j] = 1e-6;
     }
-    // with a progress callback the host regains control every few checks
-    long long pause_every = cb ? (long long)rp->check * 8 : limit;
     hc.n_pause = std::min(limit, pause_every);
     hc.done = limit == 0 ? 1 : 0;
-    AdrCtrl* dctrl = A.ctrl.as<AdrCtrl>();
-    CK(cudaMemcpyAsync(dctrl, &hc, sizeof(hc), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(A.ctrl.p, &hc, sizeof(hc), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));  // the host vector above goes out of scope
+    A.rp = *rp;
+    return PRT_OK;
+}
 
+int adr_run_finish(prt_ctx* ctx, prt_adr_result* res) {
+    AdrState& A = ctx->adr;
+    cudaStream_t s = ctx->stream;
+    AdrCtrl cur;
+    CK(cudaMemcpyAsync(&cur, A.ctrl.p, sizeof(cur), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const long long n = cur.n_base;
+    const int K = (int)A.sched.size();
+    const size_t slot_bytes = (size_t)A.d.g.n * A.p.ns * 4;
+    // keep_steps = [0] + ladder steps <= n, plus n itself when not one of them
+    A.keep_steps.clear();
+    A.slot_of_index.clear();
+    A.keep_steps.push_back(0);
+    A.slot_of_index.push_back(0);
+    for (int k = 0; k < K && A.sched[k] <= n; ++k) {
+        A.keep_steps.push_back(A.sched[k]);
+        A.slot_of_index.push_back(k + 1);
+    }
+    if (A.keep_steps.back() != n) {
+        CK(cudaMemcpyAsync(A.ladder.as<char>() + slot_bytes * (K + 1), A.buf[n & 1].p, slot_bytes,
+                           cudaMemcpyDeviceToDevice, s));
+        A.keep_steps.push_back(n);
+        A.slot_of_index.push_back(K + 1);
+    }
+    CK(cudaStreamSynchronize(s));
+    A.ran = true;
+    if (res) {
+        memset(res, 0, sizeof(*res));
+        res->steps = n;
+        res->hit_cap = (A.rp.until_conv && n >= A.rp.limit) ? 1 : 0;
+        res->ladder = (int32_t)A.keep_steps.size();
+        res->checks = cur.checks;
+        res->last_rest = cur.last_rest;
+    }
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progress_cb cb,
+                           void* user, prt_adr_result* res) {
+    if (!ctx || !rp) return fail(ctx, PRT_E_INVALID, "null argument");
+    // with a progress callback the host regains control every few checks
+    const long long pause_every = cb ? (long long)rp->check * 8 : rp->limit;
+    int rc = adr_run_setup(ctx, rp, pause_every);
+    if (rc != PRT_OK) return rc;
+    AdrState& A = ctx->adr;
+    cudaStream_t s = ctx->stream;
+    const long long limit = rp->limit;
+    const int log_cap = A.d.log_cap;
+    AdrCtrl* dctrl = A.ctrl.as<AdrCtrl>();
     const int check = rp->check;
     const prt_adr_params P = A.p;
     const AdrDev D = A.d;
@@ -801,7 +890,9 @@ extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progr
     const int per_chunk = check + 3 + (D.tree.nleaf > 0 ? 1 : 0);
     std::vector<ProgressRec> logbuf;
     int delivered = 0;
-    AdrCtrl cur = hc;
+    AdrCtrl cur;
+    CK(cudaMemcpyAsync(&cur, dctrl, sizeof(cur), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     bool use_graph = !graphs_disabled();
     if (use_graph && !cur.done) CK(build_while_graph(s, A.graph, emit));
     CK(cudaEventRecord(ctx->ev[2], s));
@@ -851,33 +942,7 @@ extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progr
         ctx->timing[2] = ms;
         ctx->timing[3] = (double)cur.n_base;
     }
-    const long long n = cur.n_base;
-    // keep_steps = [0] + ladder steps <= n, plus n itself when not one of them
-    A.keep_steps.clear();
-    A.slot_of_index.clear();
-    A.keep_steps.push_back(0);
-    A.slot_of_index.push_back(0);
-    for (int k = 0; k < K && sched[k] <= n; ++k) {
-        A.keep_steps.push_back(sched[k]);
-        A.slot_of_index.push_back(k + 1);
-    }
-    if (A.keep_steps.back() != n) {
-        CK(cudaMemcpyAsync(A.ladder.as<char>() + slot_bytes * (K + 1), A.buf[n & 1].p, slot_bytes,
-                           cudaMemcpyDeviceToDevice, s));
-        A.keep_steps.push_back(n);
-        A.slot_of_index.push_back(K + 1);
-    }
-    CK(cudaStreamSynchronize(s));
-    A.ran = true;
-    if (res) {
-        memset(res, 0, sizeof(*res));
-        res->steps = n;
-        res->hit_cap = (rp->until_conv && n >= limit) ? 1 : 0;
-        res->ladder = (int32_t)A.keep_steps.size();
-        res->checks = cur.checks;
-        res->last_rest = cur.last_rest;
-    }
-    return PRT_OK;
+    return adr_run_finish(ctx, res);
 }
 
 extern "C" int prt_adr_ladder(prt_ctx* ctx, int64_t* steps, int32_t cap, int32_t* count) {
