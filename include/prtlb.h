@@ -274,6 +274,92 @@ int prt_adr_means(prt_ctx* ctx, int32_t slot, float* means);
 /* Release the transport state of the context. */
 int prt_adr_end(prt_ctx* ctx);
 
+/* ------------------------------------------------------------------------
+ * Batched and served solves.  No counterpart in the reference, which runs
+ * one solve at a time (build_dataset_3d.py loops over rocks and calls
+ * stokes_d3q19 then solve_adr for each).  A solve is split into set-up
+ * (prt_flow_start / prt_adr_start), a time loop that a batch runs together
+ * with other solves, and results (prt_flow_finish / prt_adr_finish).  The
+ * loop of a batched solve is bit-identical to prt_flow / prt_adr_run on the
+ * same inputs, whatever else is in the batch.
+ * ------------------------------------------------------------------------ */
+
+/* Sets up the flow solve of prt_flow on ctx without running its loop; the
+ * material grid is copied from the host. */
+int prt_flow_start(prt_ctx* ctx, const uint8_t* mat, const prt_flow_params* p);
+
+/* Final field and info of a started flow solve whose loop has finished.
+ * vel_out is a host buffer as in prt_flow, or NULL to keep the field on the
+ * device only (for prt_adr_stage_flow). */
+int prt_flow_finish(prt_ctx* ctx, float* vel_out, prt_flow_info* info);
+
+/* prt_adr_stage_dev on the material grid and final field of the context's
+ * own flow solve (after prt_flow_finish). */
+int prt_adr_stage_flow(prt_ctx* ctx, const prt_adr_geom* geom, prt_adr_stats* stats);
+
+/* Frees the flow lattices and maps of ctx (keeps the material grid and the
+ * field staged for transport). */
+int prt_flow_release(prt_ctx* ctx);
+
+/* Sets up the transport run of prt_adr_run (after prt_adr_begin) without
+ * running its loop; no progress callback. */
+int prt_adr_start(prt_ctx* ctx, const prt_adr_run_params* rp);
+
+/* Result of a started transport run whose loop has finished; afterwards
+ * prt_adr_ladder / prt_adr_fetch work as after prt_adr_run. */
+int prt_adr_finish(prt_ctx* ctx, prt_adr_result* res);
+
+typedef struct prt_batch prt_batch;
+
+/* A batch on CUDA device `device`, with its own stream.  Each step advances
+ * every running job by one flow iteration or one transport step, all jobs
+ * in one persistent launch per (lattice, precision) or (dimension, species)
+ * class, over a work list of 256-voxel tiles; steps run as a CUDA graph of
+ * `graph_steps` steps (0: 20). */
+int prt_batch_create(int device, int32_t graph_steps, prt_batch** out);
+
+/* Waits for the batch's work and frees it; the jobs are left as they are. */
+void prt_batch_destroy(prt_batch* b);
+
+const char* prt_batch_last_error(const prt_batch* b);
+
+/* Adds a context whose flow solve was started (prt_flow_start) or whose
+ * transport run was started (prt_adr_start); it joins at the next launch.
+ * A context is in one batch at a time, on the batch's device, and must not
+ * be used by other calls until it is collected or removed. */
+int prt_batch_add(prt_batch* b, prt_ctx* job);
+
+/* Takes a job out of the batch (not needed for collected jobs). */
+int prt_batch_remove(prt_batch* b, prt_ctx* job);
+
+/* Enqueues `steps` batch steps and returns without waiting. */
+int prt_batch_launch(prt_batch* b, int32_t steps);
+
+/* Waits for the enqueued steps; *n_done = jobs whose loop has finished. */
+int prt_batch_wait(prt_batch* b, int32_t* n_done);
+
+/* prt_batch_launch then prt_batch_wait. */
+int prt_batch_run(prt_batch* b, int32_t steps, int32_t* n_done);
+
+/* Moves up to `cap` finished jobs out of the batch into out[] (after a
+ * wait); *count = how many. */
+int prt_batch_collect(prt_batch* b, prt_ctx** out, int32_t cap, int32_t* count);
+
+/* Jobs in the batch (pending additions included). */
+int prt_batch_size(const prt_batch* b, int32_t* flow_jobs, int32_t* adr_jobs);
+
+/* Tile size in 256-voxel blocks (1, 2 or 4) and persistent grid multiple
+ * (1 or 2 resident waves); 0, 0 = choose by timing the first launches. */
+int prt_batch_tune(prt_batch* b, int32_t tile_blocks, int32_t grid_mult);
+
+/* out8: kernel launches, graph builds, tile blocks, grid multiple, steps
+ * run, last launch ms (device), tiles of the last launch, 0. */
+int prt_batch_stats(const prt_batch* b, double* out8);
+
+/* Free and total memory of CUDA device `device` (cudaMemGetInfo), for
+ * admission control; errors via prt_last_error(NULL). */
+int prt_mem_info(int device, uint64_t* free_bytes, uint64_t* total_bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,119 @@
+// batch.cu -- the flow time loop of many solves in one launch per iteration.
+//
+// A batch holds flow solves of any sizes; their pore slots are cut into
+// 256-slot blocks and listed as tiles (job, first block, block count).  One
+// persistent launch walks the tile list and runs one LB iteration of every
+// job that is not done, each job at its own iteration count and parity.
+// The arithmetic per voxel is lb_cell_rw, the per-block |u_x| partials are
+// block_sum_store over the same 256 slots, and the convergence update is
+// flow_ctrl_advance, so a job's iterations, decisions and final field are
+// bit-identical to the single-solve loop whatever else shares the batch.
+//
+// The control block of a job advances once all its blocks are done: every
+// tile adds its block count to the job's arrival counter, and the tile that
+// completes the count sums the partials (when the iteration samples the
+// convergence mean), advances the control block and clears the counter.
+// Tiles of the same job read the control block before they arrive, so the
+// update cannot race with them.
+#include "lb_core.cuh"
+
+namespace prt {
+
+template <class L, class M>
+__global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
+    batch_flow_kernel(const FlowJob* __restrict__ jobs, const BatchTile* __restrict__ tiles,
+                      const int* __restrict__ ntiles_p) {
+    using S = typename M::S;
+    __shared__ int s_last;
+    const int ntiles = *ntiles_p;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const BatchTile tl = tiles[t];
+        const FlowJob& J = jobs[tl.job];
+        FlowCtrl* ctrl = J.ctrl;
+        const long long it = __ldcg(&ctrl->it_base);
+        if (__ldcg(&ctrl->done) || it >= __ldcg(&ctrl->nit)) continue;  // uniform over the block
+        const bool check = __ldcg(&ctrl->tol) > 0 && ((it + 1) % __ldcg(&ctrl->every)) == 0;
+        const FlowMap fm = J.fm;
+        const long long QN = (long long)L::Q * fm.nf;
+        S* f = static_cast<S*>(J.f);
+        const S* lr = (it & 1) ? f + QN : f;
+        S* lw = (it & 1) ? f : f + QN;
+        for (int b = tl.b0; b < tl.b0 + tl.nb; ++b) {
+            const int k = b * kFlowThreads + threadIdx.x;
+            double acc = 0.0;
+            if (k < fm.nf) acc = lb_cell_rw<L, M>(lr, lw, fm, J.g, J.kc, k);
+            if (check) block_sum_store(acc, J.partials + b);
+        }
+        // every warp has read the control block and finished its voxels
+        // before the tile arrives (the last arrival advances the block)
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();  // partials before the arrival
+            const unsigned old = atomicAdd(J.arrive, (unsigned)tl.nb);
+            s_last = (old + (unsigned)tl.nb == (unsigned)J.nb) ? 1 : 0;
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            const double sum = check ? block_sum_fixed(J.partials, J.nb) : 0.0;
+            if (threadIdx.x == 0) {
+                flow_ctrl_advance(ctrl, it + 1, check, sum);
+                *J.arrive = 0u;
+                __threadfence();
+            }
+        }
+        __syncthreads();  // s_last is reused by the next tile
+    }
+}
+
+template <class L, class M>
+static cudaError_t launch_batch_t(const FlowJob* jobs, const BatchTile* tiles, const int* ntiles,
+                                  int grid, cudaStream_t s) {
+    batch_flow_kernel<L, M><<<grid, kFlowThreads, 0, s>>>(jobs, tiles, ntiles);
+    return cudaGetLastError();
+}
+
+template <class L, class M>
+static int occupancy_t() {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_flow_kernel<L, M>, kFlowThreads,
+                                                      0) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return nb > 0 ? nb : 1;
+}
+
+#define PRT_BATCH_DISPATCH(FN, ...)                                                  \
+    if (nd == 3) {                                                                   \
+        if (precision == PRT_FP64) return FN<D3Q19, ModeF64>(__VA_ARGS__);           \
+        if (precision == PRT_FP32) return FN<D3Q19, ModeF32D>(__VA_ARGS__);          \
+        if (precision == PRT_FP32_F32) return FN<D3Q19, ModeF32>(__VA_ARGS__);       \
+        return FN<D3Q19, ModeF16>(__VA_ARGS__);                                      \
+    }                                                                                \
+    if (precision == PRT_FP64) return FN<D2Q9, ModeF64>(__VA_ARGS__);                \
+    if (precision == PRT_FP32) return FN<D2Q9, ModeF32D>(__VA_ARGS__);               \
+    if (precision == PRT_FP32_F32) return FN<D2Q9, ModeF32>(__VA_ARGS__);            \
+    return FN<D2Q9, ModeF16>(__VA_ARGS__);
+
+cudaError_t batch_launch_flow(int nd, int precision, const FlowJob* jobs, const BatchTile* tiles,
+                              const int* ntiles, int grid, cudaStream_t s) {
+    PRT_BATCH_DISPATCH(launch_batch_t, jobs, tiles, ntiles, grid, s)
+}
+
+int batch_flow_occupancy(int nd, int precision) { PRT_BATCH_DISPATCH(occupancy_t) }
+
+// out[i] = *done_ptrs[i]: the done flags of every job of a batch in one copy.
+__global__ void batch_status_kernel(const int* const* __restrict__ done_ptrs, int n,
+                                    int* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = *done_ptrs[i];
+}
+
+cudaError_t batch_launch_status(const int* const* done_ptrs, int n, int* out, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    batch_status_kernel<<<(n + 255) / 256, 256, 0, s>>>(done_ptrs, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace prt

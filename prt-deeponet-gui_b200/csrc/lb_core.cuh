@@ -229,22 +229,87 @@ __device__ __forceinline__ void collide_store(S* __restrict__ lw, int c, long lo
 
 constexpr int kFlowThreads = 256;
 
-// One pore voxel (slot k) of one LB iteration: gather, moments, collision,
-// store into the write lattice; returns |u_x| for the convergence mean.
-template <class L, class M, bool ODD>
-__device__ __forceinline__ double lb_cell(typename M::S* __restrict__ f, const FlowMap& fm,
-                                          const Grid& g, const LbParams& kc, int k) {
+// One pore voxel (slot k) of one LB iteration from read lattice lr into
+// write lattice lw: gather, moments, collision, store; returns |u_x| for
+// the convergence mean.
+template <class L, class M>
+__device__ __forceinline__ double lb_cell_rw(const typename M::S* __restrict__ lr,
+                                             typename M::S* __restrict__ lw, const FlowMap& fm,
+                                             const Grid& g, const LbParams& kc, int k) {
     using S = typename M::S;
     using R = typename M::R;
     using RA = typename M::RA;
-    const long long QN = (long long)L::Q * fm.nf;
-    const S* lr = ODD ? f + QN : f;
-    S* lw = ODD ? f : f + QN;
     typename Pop<S>::H h[L::Q];
     gather<L, S>(lr, lw, k, fm, g, kc.inv_scale, h);
     const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
     collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
     return fabs((double)m.jx * (double)m.inv_rho);
+}
+
+// The same with the lattice pair chosen by the iteration parity: iteration
+// t reads lattice (t & 1) and writes the other one.
+template <class L, class M, bool ODD>
+__device__ __forceinline__ double lb_cell(typename M::S* __restrict__ f, const FlowMap& fm,
+                                          const Grid& g, const LbParams& kc, int k) {
+    const long long QN = (long long)L::Q * fm.nf;
+    return lb_cell_rw<L, M>(ODD ? f + QN : f, ODD ? f : f + QN, fm, g, kc, k);
+}
+
+// Block sum of one double per thread (warp shuffles, then the warp sums in
+// order), stored by thread 0.  Both the single-solve and the batched step
+// kernels reduce |u_x| with it, so their per-block partials agree bit for
+// bit.  Every thread of the block must call it.
+__device__ __forceinline__ void block_sum_store(double acc, double* out) {
+    __shared__ double sh[kFlowThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < kFlowThreads / 32 ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) *out = v;
+    }
+    __syncthreads();
+}
+
+// Deterministic sum of n per-block partials by one block of kFlowThreads
+// threads (fixed order: strided per thread, then a shared-memory tree).
+// Loads bypass L1 because in the batched kernel other blocks of the same
+// launch wrote the partials.
+__device__ __forceinline__ double block_sum_fixed(const double* p, int n) {
+    __shared__ double sh[kFlowThreads];
+    double v = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v += __ldcg(p + i);
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// FlowConvergence bookkeeping (prtlb_3d.py:220-235) once the iterations up
+// to `end` are done; `check` says whether the mean |u_x| of iteration end-1
+// (sum s over the pore) is sampled at this point.
+__device__ __forceinline__ void flow_ctrl_advance(FlowCtrl* c, long long end, bool check,
+                                                  double s) {
+    c->iters = end;
+    if (check) {
+        const double u = c->nfluid > 0 ? s / (double)c->nfluid : 0.0;
+        if (c->has_prev) {
+            c->change = fabs(u - c->prev) / fmax(fabs(u), 1e-30);
+            if (c->change <= c->tol) c->converged = 1;
+        }
+        c->prev = u;
+        c->has_prev = 1;
+    }
+    c->it_base = end;
+    if (c->converged || end >= c->nit) c->done = 1;
 }
 
 }  // namespace prt

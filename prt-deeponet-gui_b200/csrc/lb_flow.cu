@@ -39,35 +39,7 @@ __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
         const double ux = lb_cell<L, M, ODD>(f, fm, g, kc, k);
         if (CHECK) acc = ux;
     }
-    if (CHECK) {
-        __shared__ double sh[kFlowThreads / 32];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            double v = threadIdx.x < kFlowThreads / 32 ? sh[threadIdx.x] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (threadIdx.x == 0) partials[blockIdx.x] = v;
-        }
-    }
-}
-
-// Deterministic sum of per-block partials by one block.
-__device__ double block_sum_fixed(const double* __restrict__ p, int n) {
-    __shared__ double sh[256];
-    double v = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) v += p[i];
-    sh[threadIdx.x] = v;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
-        __syncthreads();
-    }
-    double r = sh[0];
-    __syncthreads();
-    return r;
+    if (CHECK) block_sum_store(acc, partials + blockIdx.x);
 }
 
 // FlowConvergence.done() at the end of a chunk of `every` iterations
@@ -85,18 +57,7 @@ __global__ void flow_check_kernel(FlowCtrl* ctrl, const double* __restrict__ par
         if (use_handle) cudaGraphSetConditional(h, 0);
         return;
     }
-    ctrl->iters = end;
-    if (ctrl->tol > 0 && full && (end % ctrl->every) == 0) {
-        const double u = ctrl->nfluid > 0 ? s / (double)ctrl->nfluid : 0.0;
-        if (ctrl->has_prev) {
-            ctrl->change = fabs(u - ctrl->prev) / fmax(fabs(u), 1e-30);
-            if (ctrl->change <= ctrl->tol) ctrl->converged = 1;
-        }
-        ctrl->prev = u;
-        ctrl->has_prev = 1;
-    }
-    ctrl->it_base = end;
-    if (ctrl->converged || end >= ctrl->nit) ctrl->done = 1;
+    flow_ctrl_advance(ctrl, end, ctrl->tol > 0 && full && (end % ctrl->every) == 0, s);
     if (use_handle) cudaGraphSetConditional(h, ctrl->done ? 0 : 1);
 }
 

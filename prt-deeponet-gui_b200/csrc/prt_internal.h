@@ -163,4 +163,60 @@ cudaError_t adr_launch_means(const AdrDev& d, AdrCtrl* ctrl, int slot_or_neg, fl
 cudaError_t adr_launch_stop(const AdrDev& d, AdrCtrl* ctrl, const float* means,
                             cudaGraphConditionalHandle h, int use_handle, cudaStream_t s);
 
+// Batched solves (batch.cu, batch_adr.cu, engine.cu) ------------------------
+// A work-list entry: the 256-slot blocks [b0, b0 + nb) of job `job`.
+struct BatchTile {
+    int job;
+    int b0;
+    int nb;
+    int pad;
+};
+
+// One flow solve of a batch: what the single-solve kernels take as
+// arguments, plus the per-job convergence partials and an arrival counter
+// (tile blocks finished in the current iteration; the block that completes
+// the count advances the control block).
+struct FlowJob {
+    void* f;
+    FlowMap fm;
+    Grid g;
+    LbParams kc;
+    FlowCtrl* ctrl;
+    double* partials;  // one per 256-slot block, as in the single solve
+    unsigned* arrive;
+    int nb;            // 256-slot blocks of the job
+    int pad;
+};
+
+// One transport solve of a batch.
+struct AdrJob {
+    AdrDev d;
+    prt_adr_params p;
+    AdrCtrl* ctrl;
+    float* means;  // ns floats: the pore means of the latest check
+};
+
+// A leaf work-list entry: leaves [leaf0, leaf0 + 256) of species `species`
+// of transport job `job`.
+struct LeafItem {
+    int job;
+    int species;
+    int leaf0;
+    int pad;
+};
+
+// Each launch is persistent: `grid` blocks walk the work list, whose length
+// is read on the device so a captured graph stays valid when the list is
+// rewritten between replays.
+cudaError_t batch_launch_flow(int nd, int precision, const FlowJob* jobs, const BatchTile* tiles,
+                              const int* ntiles, int grid, cudaStream_t s);
+int batch_flow_occupancy(int nd, int precision);
+cudaError_t batch_launch_adr(int nd, int ns, const AdrJob* jobs, const BatchTile* tiles,
+                             const int* ntiles, int grid, cudaStream_t s);
+int batch_adr_occupancy(int nd, int ns);
+cudaError_t batch_launch_adr_leaf(const AdrJob* jobs, const LeafItem* items, const int* nitems,
+                                  int grid, cudaStream_t s);
+cudaError_t batch_launch_adr_ctrl(const AdrJob* jobs, const int* njobs, int grid, cudaStream_t s);
+cudaError_t batch_launch_status(const int* const* done_ptrs, int n, int* out, cudaStream_t s);
+
 }  // namespace prt

@@ -2,266 +2,14 @@
 // buffers, and the two time loops run as CUDA graphs with a device-side
 // while-condition, so a whole flow solve or transport solve is one graph
 // launch and the host waits once.
-#include <cuda_runtime.h>
-
-#include <algorithm>
-#include <cmath>
-#include <cstdio>
-#include <cstdlib>
-#include <cstring>
 #include <new>
-#include <string>
-#include <vector>
 
-#include "prt_internal.h"
+#include "runtime_internal.h"
 
 using namespace prt;
 
-namespace prt {
-cudaError_t adr_launch_chunk_means(const AdrDev& d, AdrCtrl* ctrl, const float** src_slot,
-                                   float* means_out, cudaStream_t s);
-cudaError_t adr_launch_flags(const uint8_t* mat, const Grid& g, int nd, int pore, int bfc,
-                             uint32_t* flags, uint8_t* mflag, cudaStream_t s);
-cudaError_t adr_launch_vel_stats(const float* vel, const AdrDev& d, float* tmp, float* means,
-                                 unsigned* vmax_bits, unsigned long long* nbf, cudaStream_t s);
-}  // namespace prt
-
 namespace {
-
 thread_local std::string g_create_error;
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    cudaError_t ensure(size_t want) {
-        if (want <= bytes && p) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-        cudaError_t e = cudaMalloc(&p, want ? want : 1);
-        if (e == cudaSuccess) bytes = want;
-        return e;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    template <class T>
-    T* as() const { return static_cast<T*>(p); }
-};
-
-struct GraphHolder {
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    bool conditional = false;
-    void release() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
-    }
-};
-
-struct FlowKey {
-    int nd = 0, precision = -1, every = 0;
-    Grid g{0, 0, 0, 0};
-    double force = 0, tau = 0, magic = 0;
-    long long nit = -1;
-    double tol = 0;
-    void* f = nullptr;
-    void* aux[4] = {nullptr, nullptr, nullptr, nullptr};
-    long long nf = -1;  // pore voxels: launch sizes and the lattice stride are baked in
-    bool operator==(const FlowKey& o) const {
-        return nd == o.nd && precision == o.precision && every == o.every && g.nx == o.g.nx &&
-               g.ny == o.g.ny && g.nz == o.g.nz && force == o.force && tau == o.tau &&
-               magic == o.magic && nit == o.nit && tol == o.tol && f == o.f && aux[0] == o.aux[0] &&
-               aux[1] == o.aux[1] && aux[2] == o.aux[2] && aux[3] == o.aux[3] && nf == o.nf;
-    }
-};
-
-struct FlowState {
-    DevBuf f, fluid, partials, ctrl, out5, count, mat, vel, flag, cnt, cells;
-    GraphHolder graph;
-    FlowKey key;
-    // the solve set up by flow_setup
-    prt_flow_params p{};
-    Grid g{0, 0, 0, 0};
-    FlowMap fm{0, nullptr, nullptr};
-    LbParams kc{};
-    int nb = 1;
-    long long nfluid = 0;
-    float scale = 1.f;
-    float* d_vel = nullptr;
-};
-
-struct AdrState {
-    bool begun = false;
-    bool ran = false;
-    prt_adr_params p{};
-    AdrDev d{};
-    DevBuf mat, vel, flags, mflag, face[3], buf[2], ladder, slot_of_step, idx, cnt, total;
-    DevBuf tree_leaf_start, tree_leaf_len, tree_inner_l, tree_inner_r, tree_level_off, tree_vals;
-    DevBuf means, src_slot, ctrl, log;
-    bool staged = false;
-    prt_adr_geom geom{};
-    const uint8_t* d_mat = nullptr;  // staged inputs (borrowed until begin)
-    const float* d_vel = nullptr;
-    DevBuf tmp, vstats;
-    std::vector<long long> sched;       // ladder step schedule of the run
-    prt_adr_run_params rp{};
-    std::vector<long long> keep_steps;  // ladder step numbers
-    std::vector<int> slot_of_index;     // ladder index -> slot
-    int nslots = 0;
-    GraphHolder graph;
-    void release() {
-        DevBuf* all[] = {&mat, &vel, &flags, &mflag, &face[0], &face[1], &face[2], &buf[0], &buf[1],
-                         &ladder, &slot_of_step, &idx, &cnt, &total, &tree_leaf_start,
-                         &tree_leaf_len, &tree_inner_l, &tree_inner_r, &tree_level_off, &tree_vals,
-                         &means, &src_slot, &ctrl, &log, &tmp, &vstats};
-        for (DevBuf* b : all) b->release();
-        staged = false;
-        graph.release();
-        keep_steps.clear();
-        slot_of_index.clear();
-        begun = ran = false;
-    }
-};
-
-}  // namespace
-
-struct prt_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    int64_t launches = 0;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    double timing[4] = {0, 0, 0, 0};
-    FlowState flow;
-    AdrState adr;
-};
-
-namespace {
-
-int fail(prt_ctx* c, int code, const std::string& msg) {
-    if (c) c->err = msg;
-    return code;
-}
-
-int cuda_fail(prt_ctx* c, cudaError_t e, const char* what) {
-    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
-    return fail(c, e == cudaErrorMemoryAllocation ? PRT_E_OOM : PRT_E_CUDA, m);
-}
-
-#define CK(expr)                                                   \
-    do {                                                           \
-        cudaError_t _e = (expr);                                   \
-        if (_e != cudaSuccess) return cuda_fail(ctx, _e, #expr);   \
-    } while (0)
-
-bool graphs_disabled() {
-    const char* v = std::getenv("PRT_GRAPHS");
-    return v && v[0] == '0';
-}
-
-// Build "while (cond) { body }" as a graph; body is captured from `emit`.
-// Falls back to a plain graph of the body when conditional nodes are
-// unavailable (the host then relaunches it until the control block says done).
-template <class Emit>
-cudaError_t build_while_graph(cudaStream_t s, GraphHolder& gh, Emit emit) {
-    gh.release();
-    cudaError_t e = cudaGraphCreate(&gh.graph, 0);
-    if (e != cudaSuccess) return e;
-    cudaGraphConditionalHandle handle;
-    e = cudaGraphConditionalHandleCreate(&handle, gh.graph, 1, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess) {
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = handle;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t node;
-        e = cudaGraphAddNode(&node, gh.graph, nullptr, 0, &cp);
-        if (e == cudaSuccess) {
-            cudaGraph_t body = cp.conditional.phGraph_out[0];
-            e = cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
-                                              cudaStreamCaptureModeThreadLocal);
-            if (e == cudaSuccess) {
-                cudaError_t ee = emit(handle, 1);
-                cudaGraph_t outg = nullptr;
-                e = cudaStreamEndCapture(s, &outg);
-                if (ee != cudaSuccess) e = ee;
-                if (e == cudaSuccess) {
-                    e = cudaGraphInstantiate(&gh.exec, gh.graph, 0);
-                    if (e == cudaSuccess) {
-                        gh.conditional = true;
-                        return cudaSuccess;
-                    }
-                }
-            }
-        }
-    }
-    // fallback: plain body graph
-    cudaGetLastError();
-    gh.release();
-    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return e;
-    cudaError_t ee = emit(cudaGraphConditionalHandle(0), 0);
-    e = cudaStreamEndCapture(s, &gh.graph);
-    if (ee != cudaSuccess) return ee;
-    if (e != cudaSuccess) return e;
-    e = cudaGraphInstantiate(&gh.exec, gh.graph, 0);
-    gh.conditional = false;
-    return e;
-}
-
-Grid make_grid(int nd, const int32_t* dims) {
-    Grid g;
-    if (nd == 3) {
-        g.nx = dims[0];
-        g.ny = dims[1];
-        g.nz = dims[2];
-    } else {
-        g.nx = dims[0];
-        g.ny = 1;
-        g.nz = dims[1];
-    }
-    g.n = (long long)g.nx * g.ny * g.nz;
-    return g;
-}
-
-void fill_lbconst(LbParams& k, int nd, double force, double tau, double magic, float scale) {
-    // _trt_minus (prtlb_3d.py:130-139)
-    const double om_p = 1.0 / tau;
-    const double lam_p = 1.0 / om_p - 0.5;
-    const double om_m = 1.0 / (magic / lam_p + 0.5);
-    k.omp = om_p;
-    k.omm = om_m;
-    k.half_g = 0.5 * force;
-    for (int p = 0; p < 9; ++p) k.guo[p] = 0.0;
-    // first member of each pair and its x component
-    if (nd == 3) {
-        // pairs (1,2) (3,4) ... (17,18); e_x of 1,7,9,11,13 is +1, of 3,5,15,17 is 0
-        const int pa[9] = {1, 3, 5, 7, 9, 11, 13, 15, 17};
-        const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
-        for (int p = 0; p < 9; ++p) {
-            const int a = pa[p];
-            const double w = a < 7 ? 1.0 / 18.0 : 1.0 / 36.0;
-            k.guo[p] = w * (1 - 0.5 * om_m) * 3.0 * force * ex[a];
-        }
-    } else {
-        const int pa[4] = {1, 2, 5, 6};
-        const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
-        for (int p = 0; p < 4; ++p) {
-            const int a = pa[p];
-            const double w = a < 5 ? 1.0 / 9.0 : 1.0 / 36.0;
-            k.guo[p] = w * (1 - 0.5 * om_m) * 3.0 * force * ex[a];
-        }
-    }
-    k.scale = scale;
-    k.inv_scale = 1.0f / scale;
-}
-
 }  // namespace
 
 // ===========================================================================
@@ -300,6 +48,7 @@ extern "C" int prt_create(int device, prt_ctx** out) {
 
 extern "C" void prt_destroy(prt_ctx* c) {
     if (!c) return;
+    batch_detach(c);
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     c->adr.release();
@@ -350,7 +99,7 @@ extern "C" size_t prt_sizeof(int which) {
 // Flow solve in three parts, so the batched engine can run many set-up
 // solves through one time loop: set-up (buffers, pore-only layout, control
 // block, constants), the time loop, and the final field with its reductions.
-int flow_setup(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p, float* d_vel) {
+int prt::flow_setup(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p, float* d_vel) {
     if (!ctx || !p || !d_mat || !d_vel) return fail(ctx, PRT_E_INVALID, "null argument");
     if (p->nd != 2 && p->nd != 3) return fail(ctx, PRT_E_INVALID, "nd must be 2 or 3");
     for (int i = 0; i < p->nd; ++i)
@@ -423,11 +172,13 @@ int flow_setup(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p, flo
     F.p = *p;
     F.g = g;
     F.nfluid = nfluid;
+    F.d_mat = d_mat;
     F.d_vel = d_vel;
+    F.field_ready = false;
     return PRT_OK;
 }
 
-int flow_finish(prt_ctx* ctx, prt_flow_info* info) {
+int prt::flow_finish(prt_ctx* ctx, prt_flow_info* info) {
     FlowState& F = ctx->flow;
     cudaStream_t s = ctx->stream;
     FlowCtrl res;
@@ -458,6 +209,7 @@ int flow_finish(prt_ctx* ctx, prt_flow_info* info) {
             F.p.force != 0 ? nu * (o5[0] / (double)F.g.n) / F.p.force : 0.0;
         info->fp16_scale = F.scale;
     }
+    F.field_ready = true;
     return PRT_OK;
 }
 
@@ -763,7 +515,7 @@ extern "C" int prt_adr_begin(prt_ctx* ctx, const prt_adr_params* p) {
 
 // Transport time loop in three parts (see flow_setup): the ladder and the
 // control block, the loop, and the kept snapshots.
-int adr_run_setup(prt_ctx* ctx, const prt_adr_run_params* rp, long long pause_every) {
+int prt::adr_run_setup(prt_ctx* ctx, const prt_adr_run_params* rp, long long pause_every) {
     if (!ctx || !rp) return fail(ctx, PRT_E_INVALID, "null argument");
     AdrState& A = ctx->adr;
     if (!A.begun) return fail(ctx, PRT_E_STATE, "prt_adr_run before prt_adr_begin");
@@ -824,7 +576,7 @@ int adr_run_setup(prt_ctx* ctx, const prt_adr_run_params* rp, long long pause_ev
     return PRT_OK;
 }
 
-int adr_run_finish(prt_ctx* ctx, prt_adr_result* res) {
+int prt::adr_run_finish(prt_ctx* ctx, prt_adr_result* res) {
     AdrState& A = ctx->adr;
     cudaStream_t s = ctx->stream;
     AdrCtrl cur;

@@ -112,6 +112,30 @@ _PROTOS = {
     "prt_adr_fetch_dev": (ctypes.c_int, [ctypes.c_void_p, c_i32, ctypes.c_void_p]),
     "prt_adr_means": (ctypes.c_int, [ctypes.c_void_p, c_i32, ctypes.POINTER(c_f32)]),
     "prt_adr_end": (ctypes.c_int, [ctypes.c_void_p]),
+    # split solves and the batch engine
+    "prt_flow_start": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(FlowParams)]),
+    "prt_flow_finish": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(FlowInfo)]),
+    "prt_adr_stage_flow": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdrGeom),
+                                          ctypes.POINTER(AdrStats)]),
+    "prt_flow_release": (ctypes.c_int, [ctypes.c_void_p]),
+    "prt_adr_start": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdrRunParams)]),
+    "prt_adr_finish": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdrResult)]),
+    "prt_batch_create": (ctypes.c_int, [ctypes.c_int, c_i32, ctypes.POINTER(ctypes.c_void_p)]),
+    "prt_batch_destroy": (None, [ctypes.c_void_p]),
+    "prt_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "prt_batch_add": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "prt_batch_remove": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "prt_batch_launch": (ctypes.c_int, [ctypes.c_void_p, c_i32]),
+    "prt_batch_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(c_i32)]),
+    "prt_batch_run": (ctypes.c_int, [ctypes.c_void_p, c_i32, ctypes.POINTER(c_i32)]),
+    "prt_batch_collect": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), c_i32,
+                                         ctypes.POINTER(c_i32)]),
+    "prt_batch_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(c_i32),
+                                      ctypes.POINTER(c_i32)]),
+    "prt_batch_tune": (ctypes.c_int, [ctypes.c_void_p, c_i32, c_i32]),
+    "prt_batch_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(c_f64)]),
+    "prt_mem_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
+                                    ctypes.POINTER(ctypes.c_uint64)]),
 }
 
 SIZEOF_ORDER = [FlowParams, FlowInfo, AdrParams, AdrRunParams, AdrResult, AdrGeom, AdrStats]

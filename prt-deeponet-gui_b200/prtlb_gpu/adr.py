@@ -286,6 +286,40 @@ def _surface_weights(m):
     return np.where(m, nface / float(2 * nd), 0.0).astype(np.float32)
 
 
+def stage_inputs(mat, vel, chem=None):
+    """The uint8 material grid (pore and biofilm kept, the rest solid), the
+    float32 (3,) + grid velocity and the AdrGeom that solve_adr stages."""
+    mat8, geom = stage_geom(mat, chem)
+    vel32 = np.asarray(vel, np.float32)
+    if vel32.shape[0] < 3:
+        pad = np.zeros((3,) + vel32.shape[1:], np.float32)
+        pad[:vel32.shape[0]] = vel32
+        vel32 = pad
+    vel32 = np.ascontiguousarray(vel32[:3])
+    return mat8, vel32, geom
+
+
+def stage_geom(mat, chem=None):
+    """The uint8 material grid and the AdrGeom of solve_adr's staging."""
+    mat = np.asarray(mat)
+    nd = mat.ndim
+    bf_code = getattr(chem, "biofilm_code", None) if chem is not None else None
+    if mat.dtype == np.uint8:
+        mat8 = np.ascontiguousarray(mat)
+    else:
+        if bf_code is not None and not 0 <= int(bf_code) < 256:
+            raise ValueError("the biofilm material code must fit in 0..255")
+        keep = (mat == PORE) | ((mat == bf_code) if bf_code is not None else False)
+        mat8 = np.where(keep, mat, SOLID).astype(np.uint8)
+    geom = _lib.AdrGeom()
+    geom.nd = nd
+    for i, n in enumerate(mat.shape):
+        geom.dims[i] = int(n)
+    geom.pore_code = PORE
+    geom.biofilm_code = -1 if bf_code is None else int(bf_code)
+    return mat8, geom
+
+
 def solve_adr(mat, vel, pe, da, n_t, n_species=2, steps=None, tol=2e-3, max_steps=100000,
               info=None, ratio=1.12, chem=None, da_abio=0.0, on_progress=None,
               *, device=None, ctx=None):
@@ -300,26 +334,7 @@ def solve_adr(mat, vel, pe, da, n_t, n_species=2, steps=None, tol=2e-3, max_step
         raise ValueError("grid must be 2D or 3D, got %dD" % nd)
     ctx = ctx or _lib.default_context(device)
     L = _lib.lib()
-    bf_code = getattr(chem, "biofilm_code", None) if chem is not None else None
-    if mat.dtype == np.uint8:
-        mat8 = np.ascontiguousarray(mat)
-    else:
-        if bf_code is not None and not 0 <= int(bf_code) < 256:
-            raise ValueError("the biofilm material code must fit in 0..255")
-        keep = (mat == PORE) | ((mat == bf_code) if bf_code is not None else False)
-        mat8 = np.where(keep, mat, SOLID).astype(np.uint8)
-    vel32 = np.asarray(vel, np.float32)
-    if vel32.shape[0] < 3:
-        pad = np.zeros((3,) + vel32.shape[1:], np.float32)
-        pad[:vel32.shape[0]] = vel32
-        vel32 = pad
-    vel32 = np.ascontiguousarray(vel32[:3])
-    geom = _lib.AdrGeom()
-    geom.nd = nd
-    for i, n in enumerate(mat.shape):
-        geom.dims[i] = int(n)
-    geom.pore_code = PORE
-    geom.biofilm_code = -1 if bf_code is None else int(bf_code)
+    mat8, vel32, geom = stage_inputs(mat, vel, chem)
     st = _lib.AdrStats()
     ctx.lock.acquire()
     try:
@@ -333,17 +348,47 @@ def solve_adr(mat, vel, pe, da, n_t, n_species=2, steps=None, tol=2e-3, max_step
         ctx.lock.release()
 
 
-def _loop(ctx, S, n_t, steps, tol, max_steps, ratio, on_progress):
-    """Begin + run on a staged context, then pick the snapshots (9.12,
-    prtlb_3d.py:1550-1568).  Returns (steps run, keep_steps, picked)."""
-    L = _lib.lib()
-    limit = int(steps) if steps is not None else int(max_steps)
+def run_params(S, steps, tol, max_steps, ratio):
+    """The run block of solve_adr's loop: a fixed step count, or the stop
+    rule with the `max_steps` cap (prtlb_3d.py:1460-1548)."""
     R = _lib.AdrRunParams()
-    R.limit = limit
+    R.limit = int(steps) if steps is not None else int(max_steps)
     R.until_conv = 1 if steps is None else 0
     R.check = S.check
     R.tol = float(tol)
     R.ratio = float(ratio)
+    return R
+
+
+def ladder_steps(ctx):
+    """Step numbers of the kept snapshots of a finished run."""
+    L = _lib.lib()
+    nkeep = ctypes.c_int32()
+    ctx.check(L.prt_adr_ladder(ctx.handle, None, 0, ctypes.byref(nkeep)))
+    ks = np.zeros(nkeep.value, np.int64)
+    ctx.check(L.prt_adr_ladder(ctx.handle, ks.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                               nkeep.value, ctypes.byref(nkeep)))
+    return ks
+
+
+def pick(ks, n, n_t):
+    """Ladder indices of the n_t output snapshots (prtlb_3d.py:1550-1568)."""
+    total = int(max(n, 1))
+    used, picked = set(), []
+    for w in _wanted_steps(total, n_t):
+        i = int(np.abs(ks - w).argmin())
+        if i in used:
+            i = _nearest_unused(i, used, len(ks))
+        used.add(i)
+        picked.append(i)
+    return picked
+
+
+def _loop(ctx, S, n_t, steps, tol, max_steps, ratio, on_progress):
+    """Begin + run on a staged context, then pick the snapshots.  Returns
+    (steps run, keep_steps, picked)."""
+    L = _lib.lib()
+    R = run_params(S, steps, tol, max_steps, ratio)
     res = _lib.AdrResult()
     err = []
 
@@ -362,27 +407,21 @@ def _loop(ctx, S, n_t, steps, tol, max_steps, ratio, on_progress):
         L.prt_adr_end(ctx.handle)
         raise err[0]
     ctx.check(rc)
-    nkeep = ctypes.c_int32()
-    ctx.check(L.prt_adr_ladder(ctx.handle, None, 0, ctypes.byref(nkeep)))
-    ks = np.zeros(nkeep.value, np.int64)
-    ctx.check(L.prt_adr_ladder(ctx.handle, ks.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
-                               nkeep.value, ctypes.byref(nkeep)))
     n = int(res.steps)
-    total = int(max(n, 1))
-    used, picked = set(), []
-    for w in _wanted_steps(total, n_t):
-        i = int(np.abs(ks - w).argmin())
-        if i in used:
-            i = _nearest_unused(i, used, len(ks))
-        used.add(i)
-        picked.append(i)
-    return n, ks, picked
+    ks = ladder_steps(ctx)
+    return n, ks, pick(ks, n, n_t)
 
 
 def _run(ctx, S, n_t, steps, tol, max_steps, info, ratio, da, da_abio, on_progress):
     """solve_adr's loop and outputs on a staged context (lock held)."""
-    L = _lib.lib()
     n, ks, picked = _loop(ctx, S, n_t, steps, tol, max_steps, ratio, on_progress)
+    return outputs(ctx, S, n_t, n, ks, picked, steps, max_steps, info, da, da_abio)
+
+
+def outputs(ctx, S, n_t, n, ks, picked, steps, max_steps, info, da, da_abio):
+    """(out, t_norm) and the info keys of a finished run (prtlb_3d.py:1565-1595);
+    ends the transport state of the context."""
+    L = _lib.lib()
     total = int(max(n, 1))
     repeated = n_t - len(set(picked))
     out = np.zeros((n_t, S.ns) + S.shape, np.float32)

@@ -1,0 +1,319 @@
+"""Batched solves: many flow + transport solves through one time loop.
+
+The reference solves one rock at a time (build_dataset_3d.py calls
+stokes_d3q19 and then solve_adr per rock).  Here a ``Batch`` holds any
+number of solves, each in its own libprtlb context; the library's batch
+engine advances all of them together, one persistent launch per class of
+jobs per step inside a CUDA graph, and a solve leaves the batch when its
+own loop has finished.  A solve's results are bit-identical to
+``stokes_d3q19`` / ``stokes_d2q9`` followed by ``solve_adr`` on the same
+arguments, whatever else shares the batch.
+
+A ``Request`` carries the arguments of both calls.  ``Batch.submit`` sets
+up its flow solve; ``Batch.advance`` runs batch steps, then moves finished
+flow solves on to their transport run (the host set-up of solve_adr, with
+the velocity field staying on the device) and finished transport runs to
+their ``Result``.
+"""
+
+import contextlib
+import ctypes
+import io
+import time
+
+import numpy as np
+
+from . import _lib
+from . import adr as _adr
+from . import flow as _flow
+
+FLOW_DEFAULTS = dict(nit=30000, force=2e-6, tau_lb=0.8, magic=3.0 / 16.0, tol=1e-6,
+                     precision="fp64")
+ADR_DEFAULTS = dict(n_species=2, steps=None, tol=2e-3, max_steps=100000, ratio=1.12, chem=None,
+                    da_abio=0.0)
+
+
+class Request(object):
+    """One solve: ``flow`` holds stokes_d3q19 / stokes_d2q9 keyword arguments
+    (nit, force, tau_lb, magic, tol, precision); ``adr`` holds solve_adr's
+    (pe, da, n_t and the optional n_species, steps, tol, max_steps, ratio,
+    chem, da_abio), or None for a flow-only solve.  ``keep_velocity`` copies
+    the velocity field to the host; ``fetch`` copies the snapshots."""
+
+    def __init__(self, mat, flow=None, adr=None, tag=None, keep_velocity=False, fetch=True):
+        self.mat = np.asarray(mat)
+        self.flow = dict(FLOW_DEFAULTS)
+        self.flow.update(flow or {})
+        if adr is not None:
+            missing = [k for k in ("pe", "da", "n_t") if k not in adr]
+            if missing:
+                raise ValueError("the transport solve needs %s" % ", ".join(missing))
+            a = dict(ADR_DEFAULTS)
+            a.update(adr)
+            adr = a
+        self.adr = adr
+        self.tag = tag
+        self.keep_velocity = bool(keep_velocity)
+        self.fetch = bool(fetch)
+
+
+class Result(object):
+    """What one solve returns: ``vel`` (host copy or None), ``flow_info`` (the
+    info dict of stokes_*), ``out`` / ``t_norm`` / ``adr_info`` (solve_adr's),
+    ``error`` (the exception that ended the solve, or None) and host clock
+    times ``t_submit``, ``t_flow`` (flow loop finished), ``t_done``."""
+
+    def __init__(self, tag):
+        self.tag = tag
+        self.vel = None
+        self.flow_info = {}
+        self.out = None
+        self.t_norm = None
+        self.adr_info = None
+        self.steps = 0
+        self.error = None
+        self.t_submit = None
+        self.t_flow = None
+        self.t_done = None
+
+    @property
+    def latency(self):
+        return None if self.t_done is None else self.t_done - self.t_submit
+
+
+class _Job(object):
+    def __init__(self, req, ctx, res):
+        self.req = req
+        self.ctx = ctx
+        self.res = res
+        self.phase = "flow"
+        self.S = None
+
+
+class Batch(object):
+    """A set of solves advanced together on one GPU.
+
+    ``graph_steps`` steps form one CUDA graph replay; ``advance(steps)``
+    enqueues whole replays.  ``quiet`` keeps the per-solve warnings of the
+    reference (iteration cap, Mach, grid Peclet) out of stdout; they are
+    kept in ``Result.flow_info['messages']`` instead."""
+
+    def __init__(self, device=0, graph_steps=20, quiet=False):
+        L = _lib.lib()
+        h = ctypes.c_void_p()
+        rc = L.prt_batch_create(int(device), int(graph_steps), ctypes.byref(h))
+        if rc != _lib.PRT_OK:
+            msg = L.prt_last_error(None)
+            raise _lib.PrtError(rc, msg.decode() if msg else "prt_batch_create failed")
+        self.handle = h
+        self.device = int(device)
+        self.graph_steps = int(graph_steps) or 20
+        self.quiet = bool(quiet)
+        self._jobs = {}
+        self._in_flight = False
+        self.finished = []
+
+    # -- library plumbing -------------------------------------------------
+    def _check(self, rc):
+        if rc != _lib.PRT_OK:
+            msg = _lib.lib().prt_batch_last_error(self.handle)
+            raise _lib.PrtError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if self.handle:
+            for job in list(self._jobs.values()):
+                job.ctx.close()
+            self._jobs.clear()
+            _lib.lib().prt_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self._jobs)
+
+    def stats(self):
+        """Kernel launches, graph builds, tile blocks, grid multiple, steps
+        run, last launch ms, tiles of the last launch."""
+        out = (ctypes.c_double * 8)()
+        self._check(_lib.lib().prt_batch_stats(self.handle, out))
+        keys = ("launches", "graph_builds", "tile_blocks", "grid_mult", "steps", "last_ms",
+                "tiles")
+        return {k: float(out[i]) for i, k in enumerate(keys)}
+
+    def tune(self, tile_blocks=0, grid_mult=0):
+        """Fix the tiling (tile_blocks 1/2/4, grid_mult 1/2) or, with 0, 0,
+        let the next launches time the candidates and keep the fastest."""
+        self._check(_lib.lib().prt_batch_tune(self.handle, int(tile_blocks), int(grid_mult)))
+
+    def _quiet(self):
+        return contextlib.redirect_stdout(io.StringIO()) if self.quiet else contextlib.nullcontext()
+
+    # -- solves -----------------------------------------------------------
+    def submit(self, req):
+        """Set up the flow solve of `req` and add it to the batch."""
+        if not isinstance(req, Request):
+            raise TypeError("submit() takes a Request")
+        res = Result(req.tag)
+        res.t_submit = time.perf_counter()
+        nd = req.mat.ndim
+        name = "3D flow" if nd == 3 else "2D flow"
+        f = req.flow
+        g, p = _flow.flow_params(req.mat, nd, name, f["nit"], f["force"], f["tau_lb"],
+                                 f["magic"], f["tol"], f["precision"])
+        ctx = _lib.Context(self.device)
+        try:
+            L = _lib.lib()
+            ctx.check(L.prt_flow_start(ctx.handle, g.ctypes.data_as(ctypes.c_void_p),
+                                       ctypes.byref(p)))
+            self._check(L.prt_batch_add(self.handle, ctx.handle))
+        except BaseException:
+            ctx.close()
+            raise
+        job = _Job(req, ctx, res)
+        self._jobs[ctx.handle.value] = job
+        return res
+
+    def launch(self, steps=None):
+        """Enqueue `steps` batch steps (default: one graph replay)."""
+        steps = self.graph_steps if steps is None else int(steps)
+        self._check(_lib.lib().prt_batch_launch(self.handle, steps))
+        self._in_flight = True
+
+    def wait(self):
+        """Wait for the enqueued steps; returns the Results completed by the
+        solves that finished in them (transport runs that follow a finished
+        flow solve are started and join the batch)."""
+        L = _lib.lib()
+        nd = ctypes.c_int32()
+        self._check(L.prt_batch_wait(self.handle, ctypes.byref(nd)))
+        self._in_flight = False
+        if nd.value == 0:
+            return []
+        handles = (ctypes.c_void_p * nd.value)()
+        cnt = ctypes.c_int32()
+        self._check(L.prt_batch_collect(self.handle, handles, nd.value, ctypes.byref(cnt)))
+        done = []
+        for i in range(cnt.value):
+            job = self._jobs.get(handles[i])
+            if job is None:
+                continue
+            try:
+                if job.phase == "flow":
+                    self._flow_done(job)
+                else:
+                    self._adr_done(job)
+            except (Exception, SystemExit) as e:  # SystemExit: a dead flow
+                job.res.error = e
+                job.phase = "done"
+            if job.phase == "done":
+                job.res.t_done = time.perf_counter()
+                job.ctx.close()
+                del self._jobs[handles[i]]
+                done.append(job.res)
+        self.finished.extend(done)
+        return done
+
+    def advance(self, steps=None):
+        """launch() then wait()."""
+        self.launch(steps)
+        return self.wait()
+
+    def run(self, max_steps=None):
+        """Advance until every solve has finished (or `max_steps` steps)."""
+        out = []
+        n = 0
+        while self._jobs and (max_steps is None or n < max_steps):
+            out.extend(self.advance())
+            n += self.graph_steps
+        return out
+
+    # -- phase changes ----------------------------------------------------
+    def _flow_done(self, job):
+        L = _lib.lib()
+        req, ctx, res = job.req, job.ctx, job.res
+        res.t_flow = time.perf_counter()
+        fi = _lib.FlowInfo()
+        vel = None
+        if req.keep_velocity or (req.adr is not None and _needs_host_stage(req)):
+            vel = np.empty((3,) + req.mat.shape, np.float32)
+        ctx.check(L.prt_flow_finish(ctx.handle,
+                                    vel.ctypes.data_as(ctypes.c_void_p) if vel is not None else None,
+                                    ctypes.byref(fi)))
+        f = req.flow
+        name = "3D flow" if req.mat.ndim == 3 else "2D flow"
+        buf = io.StringIO()
+        with contextlib.redirect_stdout(buf) if self.quiet else contextlib.nullcontext():
+            _flow.flow_report(name, fi, f["force"], f["tau_lb"], f["tol"], res.flow_info,
+                              f["precision"])
+        if self.quiet:
+            res.flow_info["messages"] = buf.getvalue()
+        if req.keep_velocity:
+            res.vel = vel
+        if req.adr is None:
+            job.phase = "done"
+            return
+        a = req.adr
+        st = _lib.AdrStats()
+        mat8, geom = _adr.stage_geom(req.mat, a["chem"])
+        if _needs_host_stage(req):
+            vel32 = np.ascontiguousarray(vel)
+            ctx.check(L.prt_adr_stage(ctx.handle, mat8.ctypes.data_as(ctypes.c_void_p),
+                                      vel32.ctypes.data_as(ctypes.c_void_p), ctypes.byref(geom),
+                                      ctypes.byref(st)))
+        else:
+            ctx.check(L.prt_adr_stage_flow(ctx.handle, ctypes.byref(geom), ctypes.byref(st)))
+        with self._quiet():
+            S = _adr.prepare(req.mat.shape, _adr.stats_dict(st), a["pe"], a["da"],
+                             n_species=a["n_species"], chem=a["chem"], da_abio=a["da_abio"],
+                             mat=req.mat)
+        job.S = S
+        ctx.check(L.prt_adr_begin(ctx.handle, ctypes.byref(S.params)))
+        ctx.check(L.prt_flow_release(ctx.handle))
+        R = _adr.run_params(S, a["steps"], a["tol"], a["max_steps"], a["ratio"])
+        ctx.check(L.prt_adr_start(ctx.handle, ctypes.byref(R)))
+        self._check(L.prt_batch_add(self.handle, ctx.handle))
+        job.phase = "adr"
+
+    def _adr_done(self, job):
+        L = _lib.lib()
+        req, ctx, res, S = job.req, job.ctx, job.res, job.S
+        a = req.adr
+        r = _lib.AdrResult()
+        ctx.check(L.prt_adr_finish(ctx.handle, ctypes.byref(r)))
+        n = int(r.steps)
+        ks = _adr.ladder_steps(ctx)
+        picked = _adr.pick(ks, n, int(a["n_t"]))
+        res.steps = n
+        res.adr_info = {}
+        if req.fetch:
+            res.out, res.t_norm = _adr.outputs(ctx, S, int(a["n_t"]), n, ks, picked, a["steps"],
+                                               a["max_steps"], res.adr_info, a["da"],
+                                               a["da_abio"])
+        else:
+            total = int(max(n, 1))
+            res.t_norm = (ks[picked].astype(np.float32) / total).astype(np.float32)
+            L.prt_adr_end(ctx.handle)
+        job.phase = "done"
+
+
+def _needs_host_stage(req):
+    """A biofilm material code makes the transport grid differ from the
+    flow's pore/solid grid, so the transport is staged from the host."""
+    chem = req.adr.get("chem") if req.adr else None
+    return chem is not None and getattr(chem, "biofilm_code", None) is not None
+
+
+def solve_batch(requests, device=0, graph_steps=20, quiet=False):
+    """Solve every Request in one batch; Results in request order."""
+    b = Batch(device=device, graph_steps=graph_steps, quiet=quiet)
+    try:
+        results = [b.submit(r) for r in requests]
+        b.run()
+        return results
+    finally:
+        b.close()

@@ -83,14 +83,15 @@ def _checked(name, fi, force, tau_lb):
               % (umax, ma), flush=True)
 
 
-def _solve(g, nd, name, nit, force, tau_lb, magic, tol, info, precision, device, ctx):
+def flow_params(g, nd, name, nit, force, tau_lb, magic, tol, precision):
+    """The uint8 grid and the prt_flow_params of one solve, with the
+    reference's refusals (tau, grid rank) raised before any work."""
     g = _material_u8(g)
     if g.ndim != nd:
         raise ValueError("%s expects a %dD material grid, got %dD" % (name, nd, g.ndim))
     trt_minus(1.0 / float(tau_lb), magic)  # the reference's tau refusal, before any work
     if precision not in _lib.PRECISIONS:
         raise ValueError("precision must be one of %s" % sorted(_lib.PRECISIONS))
-    ctx = ctx or _lib.default_context(device)
     p = _lib.FlowParams()
     p.nd = nd
     for i, n in enumerate(g.shape):
@@ -102,18 +103,30 @@ def _solve(g, nd, name, nit, force, tau_lb, magic, tol, info, precision, device,
     p.tol = float(tol)
     p.every = CHECK_EVERY
     p.precision = _lib.PRECISIONS[precision]
-    vel = np.empty((3,) + g.shape, np.float32)
-    fi = _lib.FlowInfo()
-    with ctx.lock:
-        ctx.check(_lib.lib().prt_flow(ctx.handle, g.ctypes.data_as(ctypes.c_void_p),
-                                      ctypes.byref(p), vel.ctypes.data_as(ctypes.c_void_p),
-                                      ctypes.byref(fi)))
+    return g, p
+
+
+def flow_report(name, fi, force, tau_lb, tol, info, precision):
+    """What a finished solve reports: FlowConvergence.report, the extra info
+    keys, and _checked_flow's refusals and warning."""
     _report(name, CHECK_EVERY, float(tol), fi, info)
     if info is not None:
         info["permeability"] = float(fi.permeability)
         info["flow_mass"] = float(fi.mass)
         info["flow_precision"] = precision
     _checked("flow", fi, force, tau_lb)
+
+
+def _solve(g, nd, name, nit, force, tau_lb, magic, tol, info, precision, device, ctx):
+    g, p = flow_params(g, nd, name, nit, force, tau_lb, magic, tol, precision)
+    ctx = ctx or _lib.default_context(device)
+    vel = np.empty((3,) + g.shape, np.float32)
+    fi = _lib.FlowInfo()
+    with ctx.lock:
+        ctx.check(_lib.lib().prt_flow(ctx.handle, g.ctypes.data_as(ctypes.c_void_p),
+                                      ctypes.byref(p), vel.ctypes.data_as(ctypes.c_void_p),
+                                      ctypes.byref(fi)))
+    flow_report(name, fi, force, tau_lb, tol, info, precision)
     return vel
 
 
