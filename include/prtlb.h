@@ -360,6 +360,21 @@ int prt_batch_stats(const prt_batch* b, double* out8);
  * admission control; errors via prt_last_error(NULL). */
 int prt_mem_info(int device, uint64_t* free_bytes, uint64_t* total_bytes);
 
+/* Host helper, no GPU: the placement loop of the seeded ball packs used as
+ * synthetic rocks (prtlb_gpu.geometry.random_pack).  No counterpart in the
+ * reference (its build_spheres, build_geometry_3d.py:129-150, makes
+ * overlapping spheres).  solid: uint8 grid of `shape` (nd 2 or 3) to stamp;
+ * cand: ncand rows of nd+1 uniform numbers (centre / L, radius fraction);
+ * centres (cap x nd) / radii (cap) hold the placed balls; state = {balls,
+ * consecutive rejections, tries, solid voxels}, read and updated.  Places
+ * until the solid fraction reaches target_frac, the tries reach max_tries,
+ * the candidates run out or `cap` balls are placed.  Returns the candidates
+ * consumed, or a negative status. */
+int64_t prt_pack_balls(uint8_t* solid, int32_t nd, const int32_t* shape, const double* cand,
+                       int64_t ncand, double rmin, double rmax, double target_frac,
+                       int64_t overlap_after, int64_t max_tries, double* centres,
+                       double* radii, int64_t cap, int64_t* state);
+
 #ifdef __cplusplus
 }
 #endif

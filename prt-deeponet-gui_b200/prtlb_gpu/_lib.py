@@ -136,6 +136,9 @@ _PROTOS = {
     "prt_batch_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(c_f64)]),
     "prt_mem_info": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                     ctypes.POINTER(ctypes.c_uint64)]),
+    "prt_pack_balls": (c_i64, [ctypes.c_void_p, c_i32, ctypes.POINTER(c_i32), ctypes.c_void_p,
+                               c_i64, c_f64, c_f64, c_f64, c_i64, c_i64, ctypes.c_void_p,
+                               ctypes.c_void_p, c_i64, ctypes.POINTER(c_i64)]),
 }
 
 SIZEOF_ORDER = [FlowParams, FlowInfo, AdrParams, AdrRunParams, AdrResult, AdrGeom, AdrStats]

@@ -92,3 +92,15 @@ def test_check_physics_rules():
     neg = good.copy()
     neg[-1, 0, 3, 3] = -0.5
     assert any("negative" in s for s in check_physics(neg, g))
+
+
+def test_native_pack_loop_matches_numpy_loop():
+    """prt_pack_balls places exactly the balls of the NumPy loop (jammed
+    packs included, where overlaps are accepted)."""
+    import numpy as np
+    from prtlb_gpu.geometry import random_pack
+    for shp, phi, a, b, sd in (((24, 20, 18), 0.45, 2.0, 4.0, 0), ((40, 40), 0.5, 2.0, 5.0, 3),
+                               ((16, 16, 16), 0.3, 1.5, 3.0, 7), ((9, 30), 0.6, 1.0, 5.5, 1)):
+        g1 = random_pack(shp, phi, a, b, seed=sd, overlap_after=300)
+        g2 = random_pack(shp, phi, a, b, seed=sd, overlap_after=300, native=False)
+        assert np.array_equal(g1, g2), shp
