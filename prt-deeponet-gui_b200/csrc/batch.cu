@@ -20,49 +20,56 @@
 namespace prt {
 
 template <class L, class M>
-__global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
+__global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
     batch_flow_kernel(const FlowJob* __restrict__ jobs, const BatchTile* __restrict__ tiles,
                       const int* __restrict__ ntiles_p) {
     using S = typename M::S;
     __shared__ int s_last;
+    __shared__ FlowJob sj;  // the tile's job: constants read where they are used
     const int ntiles = *ntiles_p;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const BatchTile tl = tiles[t];
-        const FlowJob& J = jobs[tl.job];
-        FlowCtrl* ctrl = J.ctrl;
+        if (threadIdx.x == 0) sj = jobs[tl.job];
+        __syncthreads();
+        FlowCtrl* ctrl = sj.ctrl;
         const long long it = __ldcg(&ctrl->it_base);
-        if (__ldcg(&ctrl->done) || it >= __ldcg(&ctrl->nit)) continue;  // uniform over the block
+        const bool run = !__ldcg(&ctrl->done) && it < __ldcg(&ctrl->nit);
         const bool check = __ldcg(&ctrl->tol) > 0 && ((it + 1) % __ldcg(&ctrl->every)) == 0;
-        const FlowMap fm = J.fm;
-        const long long QN = (long long)L::Q * fm.nf;
-        S* f = static_cast<S*>(J.f);
+        if (!run) {  // uniform over the block
+            __syncthreads();  // sj is rewritten by the next tile
+            continue;
+        }
+        const int nf = sj.fm.nf;
+        const long long QN = (long long)L::Q * nf;
+        S* f = static_cast<S*>(sj.f);
         const S* lr = (it & 1) ? f + QN : f;
         S* lw = (it & 1) ? f : f + QN;
+#pragma unroll 1
         for (int b = tl.b0; b < tl.b0 + tl.nb; ++b) {
             const int k = b * kFlowThreads + threadIdx.x;
             double acc = 0.0;
-            if (k < fm.nf) acc = lb_cell_rw<L, M>(lr, lw, fm, J.g, J.kc, k);
-            if (check) block_sum_store(acc, J.partials + b);
+            if (k < nf) acc = lb_cell_rw<L, M>(lr, lw, sj.fm, sj.g, sj.kc, k);
+            if (check) block_sum_store(acc, sj.partials + b);
         }
         // every warp has read the control block and finished its voxels
         // before the tile arrives (the last arrival advances the block)
         __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();  // partials before the arrival
-            const unsigned old = atomicAdd(J.arrive, (unsigned)tl.nb);
-            s_last = (old + (unsigned)tl.nb == (unsigned)J.nb) ? 1 : 0;
+            const unsigned old = atomicAdd(sj.arrive, (unsigned)tl.nb);
+            s_last = (old + (unsigned)tl.nb == (unsigned)sj.nb) ? 1 : 0;
         }
         __syncthreads();
         if (s_last) {
             __threadfence();
-            const double sum = check ? block_sum_fixed(J.partials, J.nb) : 0.0;
+            const double sum = check ? block_sum_fixed(sj.partials, sj.nb) : 0.0;
             if (threadIdx.x == 0) {
                 flow_ctrl_advance(ctrl, it + 1, check, sum);
-                *J.arrive = 0u;
+                *sj.arrive = 0u;
                 __threadfence();
             }
         }
-        __syncthreads();  // s_last is reused by the next tile
+        __syncthreads();  // s_last and sj are reused by the next tile
     }
 }
 

@@ -96,30 +96,40 @@ struct Pop<__half> {
 // Precision modes: storage type S, arithmetic R for the symmetric part and
 // RA for the momentum and the antisymmetric non-equilibrium part (a small
 // difference of two O(u) numbers), and the resident 256-thread blocks per SM
-// the register budget is cut for.
+// the register budget is cut for (single-solve and batched step kernels).
+// `staged`: the arrived populations go to shared memory by cp.async, so no
+// register waits on a gather load (4- and 8-byte populations only).
 struct ModeF64 {  // the reference's arithmetic
     using S = double;
     using R = double;
     using RA = double;
-    static constexpr int min_blocks = 2;
+    static constexpr int min_blocks = 3;
+    static constexpr int batch_min_blocks = 3;
+    static constexpr bool staged = true;
 };
 struct ModeF32 {  // float32 populations, float32 collision
     using S = float;
     using R = float;
     using RA = float;
-    static constexpr int min_blocks = 3;
+    static constexpr int min_blocks = 5;
+    static constexpr int batch_min_blocks = 4;
+    static constexpr bool staged = true;
 };
 struct ModeF32D {  // float32 populations, float64 momentum
     using S = float;
     using R = float;
     using RA = double;
-    static constexpr int min_blocks = 3;
+    static constexpr int min_blocks = 5;
+    static constexpr int batch_min_blocks = 4;
+    static constexpr bool staged = true;
 };
 struct ModeF16 {  // scaled float16 populations, float32 collision
     using S = __half;
     using R = float;
     using RA = float;
     static constexpr int min_blocks = 3;
+    static constexpr int batch_min_blocks = 3;
+    static constexpr bool staged = false;
 };
 
 // Gather the arrived populations of pore voxel number k (see the file
@@ -154,6 +164,59 @@ __device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __rest
     }
 }
 
+constexpr int kFlowThreads = 256;
+
+// cp.async of one 4- or 8-byte population into this thread's shared slot.
+template <class S>
+__device__ __forceinline__ void cp_async_pop(S* dst, const S* src) {
+    static_assert(sizeof(S) == 4 || sizeof(S) == 8, "cp.async copies 4 or 8 bytes here");
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (sizeof(S) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// The arrived populations of one thread in shared memory: element i of the
+// thread's column (stride kFlowThreads).
+template <class S>
+struct Staged {
+    const S* col;
+    __device__ S operator[](int i) const { return col[i * kFlowThreads]; }
+};
+
+// gather() with the population loads issued as cp.async into `col` (this
+// thread's column of a [Q][kFlowThreads] shared array): the same sources,
+// but no register is held while a load is in flight.
+template <class L, class S>
+__device__ __forceinline__ void gather_staged(const S* __restrict__ lr, const S* __restrict__ lw,
+                                              int k, const FlowMap& fm, const Grid& g, S* col) {
+    const long long NF = fm.nf;
+    const int v = fm.cells[k];
+    const int z = v % g.nz;
+    const int t = v / g.nz;
+    const int y = t % g.ny;
+    const int x = t / g.ny;
+    const int syz = g.ny * g.nz;
+    cp_async_pop(col, lr + k);
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        const int dx = -L::c(i, 0), dy = -L::c(i, 1), dz = -L::c(i, 2);
+        int xx = x + dx, yy = y + dy, zz = z + dz;
+        if (dx) xx = xx < 0 ? g.nx - 1 : (xx >= g.nx ? 0 : xx);
+        if (dy) yy = yy < 0 ? g.ny - 1 : (yy >= g.ny ? 0 : yy);
+        if (dz) zz = zz < 0 ? g.nz - 1 : (zz >= g.nz ? 0 : zz);
+        const int src = fm.imap[xx * syz + yy * g.nz + zz];
+        const S* p = src >= 0 ? lr + (long long)i * NF + src : lw + (long long)L::opp(i) * NF + k;
+        cp_async_pop(col + i * kFlowThreads, p);
+    }
+    cp_async_wait_all();
+}
+
 template <class R, class RA>
 struct Moments {
     R drho, jsq;    // density deviation, rho u^2
@@ -163,8 +226,8 @@ struct Moments {
 
 // Moments of the arrived (shifted) populations (prtlb_3d.py:428-433):
 // drho = sum h, J = rho u = sum e h + g/2 x.
-template <class L, class R, class RA, class H>
-__device__ __forceinline__ Moments<R, RA> moments(const H (&h)[L::Q], double half_g) {
+template <class L, class R, class RA, class HA>
+__device__ __forceinline__ Moments<R, RA> moments(const HA& h, double half_g) {
     Moments<R, RA> m;
     RA s = RA(h[0]);
     RA jx = RA(0), jy = RA(0), jz = RA(0);
@@ -196,10 +259,10 @@ __device__ __forceinline__ Moments<R, RA> moments(const H (&h)[L::Q], double hal
 // antisymmetric equilibrium (w rho 3 e.u = 3 w e.J) and rho u u = J J / rho in
 // the symmetric one.  The new population is h + delta with delta summed
 // first, so the stored result rounds once; it goes to slot i of voxel c.
-template <class L, class S, class R, class RA>
+template <class L, class S, class R, class RA, class HA>
 __device__ __forceinline__ void collide_store(S* __restrict__ lw, int c, long long N,
-                                              const typename Pop<S>::H (&h)[L::Q],
-                                              const Moments<R, RA>& m, const LbParams& kc) {
+                                              const HA& h, const Moments<R, RA>& m,
+                                              const LbParams& kc) {
     const R omp = R(kc.omp);
     const R inv_rho = R(m.inv_rho);
     const R heq0 = R(L::w(0)) * (m.drho - R(1.5) * m.jsq);
@@ -227,8 +290,6 @@ __device__ __forceinline__ void collide_store(S* __restrict__ lw, int c, long lo
     }
 }
 
-constexpr int kFlowThreads = 256;
-
 // One pore voxel (slot k) of one LB iteration from read lattice lr into
 // write lattice lw: gather, moments, collision, store; returns |u_x| for
 // the convergence mean.
@@ -239,11 +300,21 @@ __device__ __forceinline__ double lb_cell_rw(const typename M::S* __restrict__ l
     using S = typename M::S;
     using R = typename M::R;
     using RA = typename M::RA;
-    typename Pop<S>::H h[L::Q];
-    gather<L, S>(lr, lw, k, fm, g, kc.inv_scale, h);
-    const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
-    collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
-    return fabs((double)m.jx * (double)m.inv_rho);
+    if constexpr (M::staged) {
+        __shared__ S stage[L::Q * kFlowThreads];
+        S* col = stage + threadIdx.x;
+        gather_staged<L, S>(lr, lw, k, fm, g, col);
+        const Staged<S> h{col};
+        const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
+        collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
+        return fabs((double)m.jx * (double)m.inv_rho);
+    } else {
+        typename Pop<S>::H h[L::Q];
+        gather<L, S>(lr, lw, k, fm, g, kc.inv_scale, h);
+        const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
+        collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
+        return fabs((double)m.jx * (double)m.inv_rho);
+    }
 }
 
 // The same with the lattice pair chosen by the iteration parity: iteration

@@ -61,7 +61,8 @@ class Result(object):
     """What one solve returns: ``vel`` (host copy or None), ``flow_info`` (the
     info dict of stokes_*), ``out`` / ``t_norm`` / ``adr_info`` (solve_adr's),
     ``error`` (the exception that ended the solve, or None) and host clock
-    times ``t_submit``, ``t_flow`` (flow loop finished), ``t_done``."""
+    times ``t_submit``, ``t_flow`` (flow loop finished), ``t_done``; a
+    served request also has ``t_arrive`` and ``t_admit``."""
 
     def __init__(self, tag):
         self.tag = tag
@@ -75,6 +76,8 @@ class Result(object):
         self.t_submit = None
         self.t_flow = None
         self.t_done = None
+        self.t_arrive = None
+        self.t_admit = None
 
     @property
     def latency(self):
@@ -110,6 +113,8 @@ class Batch(object):
         self.graph_steps = int(graph_steps) or 20
         self.quiet = bool(quiet)
         self._jobs = {}
+        self._ready = []      # collected solves waiting for their host work
+        self._graveyard = []  # finished contexts, freed when the device is idle
         self._in_flight = False
         self.finished = []
 
@@ -124,6 +129,8 @@ class Batch(object):
             for job in list(self._jobs.values()):
                 job.ctx.close()
             self._jobs.clear()
+            self._ready = []
+            self._bury()
             _lib.lib().prt_batch_destroy(self.handle)
             self.handle = None
 
@@ -134,6 +141,7 @@ class Batch(object):
             pass
 
     def __len__(self):
+        """Solves not finished yet (in the batch or waiting for host work)."""
         return len(self._jobs)
 
     def stats(self):
@@ -184,24 +192,35 @@ class Batch(object):
         self._check(_lib.lib().prt_batch_launch(self.handle, steps))
         self._in_flight = True
 
-    def wait(self):
-        """Wait for the enqueued steps; returns the Results completed by the
-        solves that finished in them (transport runs that follow a finished
-        flow solve are started and join the batch)."""
+    def wait(self, process=True):
+        """Wait for the enqueued steps and collect the solves whose loop
+        finished in them.  With process=True (default) their host work is
+        done at once (see process()) and the Results completed now are
+        returned; with process=False it is left for process(), so a caller
+        can overlap it with the next launch."""
         L = _lib.lib()
         nd = ctypes.c_int32()
         self._check(L.prt_batch_wait(self.handle, ctypes.byref(nd)))
         self._in_flight = False
-        if nd.value == 0:
-            return []
-        handles = (ctypes.c_void_p * nd.value)()
-        cnt = ctypes.c_int32()
-        self._check(L.prt_batch_collect(self.handle, handles, nd.value, ctypes.byref(cnt)))
+        self._bury()  # the device is idle: freeing memory costs no stall now
+        if nd.value:
+            handles = (ctypes.c_void_p * nd.value)()
+            cnt = ctypes.c_int32()
+            self._check(L.prt_batch_collect(self.handle, handles, nd.value, ctypes.byref(cnt)))
+            for i in range(cnt.value):
+                job = self._jobs.get(handles[i])
+                if job is not None:
+                    self._ready.append(job)
+        return self.process() if process else []
+
+    def process(self):
+        """Host work of the collected solves: a finished flow solve gets its
+        field and report and starts its transport run (which joins the
+        batch); a finished transport run gets its snapshots.  Returns the
+        Results completed."""
         done = []
-        for i in range(cnt.value):
-            job = self._jobs.get(handles[i])
-            if job is None:
-                continue
+        ready, self._ready = self._ready, []
+        for job in ready:
             try:
                 if job.phase == "flow":
                     self._flow_done(job)
@@ -212,11 +231,18 @@ class Batch(object):
                 job.phase = "done"
             if job.phase == "done":
                 job.res.t_done = time.perf_counter()
-                job.ctx.close()
-                del self._jobs[handles[i]]
+                del self._jobs[job.ctx.handle.value]
+                self._graveyard.append(job.ctx)
                 done.append(job.res)
+        if not self._in_flight:
+            self._bury()
         self.finished.extend(done)
         return done
+
+    def _bury(self):
+        for ctx in self._graveyard:
+            ctx.close()
+        self._graveyard = []
 
     def advance(self, steps=None):
         """launch() then wait()."""
