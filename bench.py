@@ -279,6 +279,125 @@ def run_ours(args, rank, world, torch, dist):
 
 
 # ---------------------------------------------------------------------------
+# batched and served modes (solves per hour; not the default bench line)
+# ---------------------------------------------------------------------------
+def plain_solve(req, ctx):
+    """One request through the drop-in single-solve API, one after another:
+    the plain per-geometry GPU path the batched and served forms are
+    compared with.  Returns (out, t_norm) or the exception that ended it."""
+    from prtlb_gpu import solve_adr, stokes_d3q19
+    f = dict(req.flow)
+    prec = f.pop("precision")
+    a = dict(req.adr)
+    try:
+        with contextlib.redirect_stdout(io.StringIO()):
+            v = stokes_d3q19(req.mat, precision=prec, ctx=ctx, **f)
+            return solve_adr(req.mat, v, a.pop("pe"), a.pop("da"), a.pop("n_t"), ctx=ctx, **a)
+    except (Exception, SystemExit) as e:
+        return e
+
+
+def _same(res, ref):
+    if isinstance(ref, BaseException) or res.error is not None:
+        return isinstance(ref, BaseException) and res.error is not None
+    return bool(np.array_equal(res.out, ref[0]) and np.array_equal(res.t_norm, ref[1]))
+
+
+def run_batched(args, torch):
+    """48 uneven geometries (edges 24-96): the batch engine against the same
+    solves one at a time."""
+    from prtlb_gpu import _lib
+    from prtlb_gpu.batch import solve_batch
+    from prtlb_gpu.workloads import batched_set
+    t = time.perf_counter()
+    reqs, draws = batched_set(args.requests, seed=SEED)
+    gen_s = time.perf_counter() - t
+    small, _ = batched_set(2, seed=SEED + 1, nit=200, max_steps=200)
+    ctx = _lib.Context(0)
+    for _ in range(args.warmup):  # warm-up: libraries, graphs, allocator
+        [plain_solve(r, ctx) for r in small]
+        solve_batch(small, quiet=True)
+    torch.cuda.synchronize()
+    with Clocks(0) as clk:
+        t0 = time.perf_counter()
+        res = solve_batch(reqs, quiet=True)
+        torch.cuda.synchronize()
+        t_batch = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ref = [plain_solve(r, ctx) for r in reqs]
+        torch.cuda.synchronize()
+        t_plain = time.perf_counter() - t0
+    ctx.close()
+    n = len(reqs)
+    same = all(_same(a, b) for a, b in zip(res, ref))
+    cells = sum(int(r.mat.size) for r in reqs)
+    return {"metric": "batched solves/h", "value": n / t_batch * 3600.0, "unit": "solves/h",
+            "n_gpus": 1, "steps": 1, "warmup": args.warmup, "ms_per_step": t_batch * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "batched: %d sphere packs, edge U{24..96}, porosity U[0.35,0.6],"
+                                   " Pe logU[0.1,100], Da logU[0.01,10], kinetics Monod / first "
+                                   "order / reversible sorption, D3Q19 fp32 to tol 1e-6 (cap "
+                                   "30000) + ADR to the stop rule (cap 100000)" % n,
+                       "voxels": cells, "seed": SEED, "geometry_s": round(gen_s, 2)},
+            "plain": {"solves_per_hour": n / t_plain * 3600.0, "seconds": t_plain},
+            "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": same,
+            "failed": sum(1 for r in res if r.error is not None), "clocks": clk.summary()}
+
+
+def run_served(args, torch):
+    """A Poisson stream of requests (edges 32-160) through the served loop,
+    against the same stream through the plain path one at a time (first
+    come, first served)."""
+    from prtlb_gpu import _lib
+    from prtlb_gpu.batch import solve_batch
+    from prtlb_gpu.serve import poisson_arrivals, serve
+    from prtlb_gpu.workloads import batched_set, served_set
+    t = time.perf_counter()
+    reqs, draws = served_set(args.requests, seed=SEED)
+    gen_s = time.perf_counter() - t
+    arrivals = poisson_arrivals(len(reqs), args.rate, seed=SEED)
+    small, _ = batched_set(2, seed=SEED + 1, nit=200, max_steps=200)
+    ctx = _lib.Context(0)
+    for _ in range(args.warmup):
+        [plain_solve(r, ctx) for r in small]
+        solve_batch(small, quiet=True)
+    torch.cuda.synchronize()
+    with Clocks(0) as clk:
+        srv = serve(reqs, arrivals)
+        torch.cuda.synchronize()
+        # plain: one server, first come first served, same arrival times
+        t0 = time.perf_counter()
+        lat, ref = [], [None] * len(reqs)
+        for i in np.argsort(arrivals, kind="stable"):
+            now = time.perf_counter() - t0
+            if now < arrivals[i]:
+                time.sleep(arrivals[i] - now)
+            ref[i] = plain_solve(reqs[i], ctx)
+            lat.append(time.perf_counter() - t0 - arrivals[i])
+        t_plain = time.perf_counter() - t0
+    ctx.close()
+    byreq = {r.tag: r for r in srv.results}
+    same = all(_same(byreq[i], ref[i]) for i in range(len(reqs)))
+    S = srv.summary
+    n = len(reqs)
+    return {"metric": "served solves/h", "value": S["solves_per_hour"], "unit": "solves/h",
+            "n_gpus": 1, "steps": 1, "warmup": args.warmup, "ms_per_step": S["makespan_s"] * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "served: %d requests, Poisson %.3g req/s, edge U{32..160}, "
+                                   "draws as the batched set, 80%% HBM admission" % (n, args.rate),
+                       "seed": SEED, "geometry_s": round(gen_s, 2)},
+            "latency_p50_s": S["latency_p50_s"], "latency_p99_s": S["latency_p99_s"],
+            "queue_p50_s": S["queue_p50_s"], "completed": S["completed"], "failed": S["failed"],
+            "plain": {"solves_per_hour": n / t_plain * 3600.0, "seconds": t_plain,
+                      "latency_p50_s": float(np.percentile(lat, 50)),
+                      "latency_p99_s": float(np.percentile(lat, 99))},
+            "speedup_vs_plain": (S["solves_per_hour"] * t_plain) / (n * 3600.0),
+            "identical_to_plain": same, "clocks": clk.summary()}
+
+
+# ---------------------------------------------------------------------------
 # CPU: the oracle (a restatement of the reference's NumPy algorithm)
 # ---------------------------------------------------------------------------
 def cpu_sample(args_tuple):
@@ -330,7 +449,17 @@ def main():
     ap.add_argument("--edge", type=int, default=64)
     ap.add_argument("--flow-nit", type=int, default=30000)
     ap.add_argument("--adr-steps", type=int, default=None)
+    # solves-per-hour modes (each prints its own line; the default is the
+    # plain 3D bench line)
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"])
+    ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--rate", type=float, default=20.0)
     args = ap.parse_args()
+    if args.mode != "plain" and args.impl == "ours":
+        import torch
+        fn = run_batched if args.mode == "batched" else run_served
+        print(json.dumps(fn(args, torch)))
+        return
     globals().update(EDGE=args.edge, FLOW_NIT=args.flow_nit, ADR_STEPS=args.adr_steps)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

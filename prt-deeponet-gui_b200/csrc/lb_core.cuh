@@ -132,6 +132,25 @@ struct ModeF16 {  // scaled float16 populations, float32 collision
     static constexpr bool staged = false;
 };
 
+// Slots of the upstream voxels x - e_i of pore slot k (periodic), -1 where
+// that voxel is rock.  The three candidate coordinates per axis are formed
+// once; each direction then costs one index and one imap load.
+template <class L>
+__device__ __forceinline__ void upstream_slots(const FlowMap& fm, const Grid& g, int k,
+                                               int (&src)[L::Q]) {
+    int x, y, z;
+    unpack_cell((unsigned)fm.cells[k], fm, x, y, z);
+    const int X[3] = {x == 0 ? g.nx - 1 : x - 1, x, x == g.nx - 1 ? 0 : x + 1};
+    const int Y[3] = {y == 0 ? g.ny - 1 : y - 1, y, y == g.ny - 1 ? 0 : y + 1};
+    const int Z[3] = {z == 0 ? g.nz - 1 : z - 1, z, z == g.nz - 1 ? 0 : z + 1};
+    src[0] = k;
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) {
+        const int a = 1 - L::c(i, 0), b = 1 - L::c(i, 1), c = 1 - L::c(i, 2);
+        src[i] = fm.imap[(X[a] * g.ny + Y[b]) * g.nz + Z[c]];
+    }
+}
+
 // Gather the arrived populations of pore voxel number k (see the file
 // comment).  Lattices hold the pore voxels only, in C order: voxel
 // cells[k] is slot k, and imap[voxel] is the slot of a pore voxel or -1.
@@ -140,22 +159,8 @@ __device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __rest
                                        const FlowMap& fm, const Grid& g, float inv,
                                        typename Pop<S>::H (&h)[L::Q]) {
     const long long NF = fm.nf;
-    const int v = fm.cells[k];
-    const int z = v % g.nz;
-    const int t = v / g.nz;
-    const int y = t % g.ny;
-    const int x = t / g.ny;
-    const int syz = g.ny * g.nz;
     int src[L::Q];
-#pragma unroll
-    for (int i = 1; i < L::Q; ++i) {
-        const int dx = -L::c(i, 0), dy = -L::c(i, 1), dz = -L::c(i, 2);
-        int xx = x + dx, yy = y + dy, zz = z + dz;
-        if (dx) xx = xx < 0 ? g.nx - 1 : (xx >= g.nx ? 0 : xx);
-        if (dy) yy = yy < 0 ? g.ny - 1 : (yy >= g.ny ? 0 : yy);
-        if (dz) zz = zz < 0 ? g.nz - 1 : (zz >= g.nz ? 0 : zz);
-        src[i] = fm.imap[xx * syz + yy * g.nz + zz];
-    }
+    upstream_slots<L>(fm, g, k, src);
     h[0] = Pop<S>::ld(lr + k, inv);
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
@@ -196,22 +201,13 @@ template <class L, class S>
 __device__ __forceinline__ void gather_staged(const S* __restrict__ lr, const S* __restrict__ lw,
                                               int k, const FlowMap& fm, const Grid& g, S* col) {
     const long long NF = fm.nf;
-    const int v = fm.cells[k];
-    const int z = v % g.nz;
-    const int t = v / g.nz;
-    const int y = t % g.ny;
-    const int x = t / g.ny;
-    const int syz = g.ny * g.nz;
+    int src[L::Q];
+    upstream_slots<L>(fm, g, k, src);
     cp_async_pop(col, lr + k);
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
-        const int dx = -L::c(i, 0), dy = -L::c(i, 1), dz = -L::c(i, 2);
-        int xx = x + dx, yy = y + dy, zz = z + dz;
-        if (dx) xx = xx < 0 ? g.nx - 1 : (xx >= g.nx ? 0 : xx);
-        if (dy) yy = yy < 0 ? g.ny - 1 : (yy >= g.ny ? 0 : yy);
-        if (dz) zz = zz < 0 ? g.nz - 1 : (zz >= g.nz ? 0 : zz);
-        const int src = fm.imap[xx * syz + yy * g.nz + zz];
-        const S* p = src >= 0 ? lr + (long long)i * NF + src : lw + (long long)L::opp(i) * NF + k;
+        const S* p = src[i] >= 0 ? lr + (long long)i * NF + src[i]
+                                 : lw + (long long)L::opp(i) * NF + k;
         cp_async_pop(col + i * kFlowThreads, p);
     }
     cp_async_wait_all();

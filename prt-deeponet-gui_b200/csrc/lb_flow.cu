@@ -81,7 +81,9 @@ __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
     double sux = 0.0, srho = 0.0, ssp = 0.0, mx = 0.0, nonf = 0.0;
     if (kk < fm.nf) {
         // solid voxels of vel were zeroed before this launch
-        const int c = fm.cells[kk];
+        int cx, cy, cz;
+        unpack_cell((unsigned)fm.cells[kk], fm, cx, cy, cz);
+        const long long c = ((long long)cx * g.ny + cy) * g.nz + cz;
         float vx = 0.f, vy = 0.f, vz = 0.f;
         {
             typename Pop<S>::H h[L::Q];
@@ -173,10 +175,19 @@ __global__ void fluid_flag_kernel(const uint8_t* __restrict__ mat, long long n, 
 }
 
 // imap[cells[k]] = k (imap was filled with -1 first).
-__global__ void imap_scatter_kernel(const int* __restrict__ cells, int nf,
-                                    int* __restrict__ imap) {
+// imap[cells[k]] = k (imap was filled with -1 first); then cells[k] is
+// rewritten from the voxel index to the packed coordinates.
+__global__ void imap_scatter_kernel(int* __restrict__ cells, int nf, int* __restrict__ imap,
+                                    Grid g, int ys, int xs) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < nf) imap[cells[k]] = k;
+    if (k >= nf) return;
+    const int v = cells[k];
+    imap[v] = k;
+    const int z = v % g.nz;
+    const int t = v / g.nz;
+    const int y = t % g.ny;
+    const int x = t / g.ny;
+    cells[k] = (int)(((unsigned)x << xs) | ((unsigned)y << ys) | (unsigned)z);
 }
 
 // -------------------------------------------------------------------------
@@ -244,9 +255,10 @@ cudaError_t flow_launch_flags(const uint8_t* mat, long long n, int pore, uint8_t
     return cudaGetLastError();
 }
 
-cudaError_t flow_launch_imap(const int* cells, int nf, int* imap, cudaStream_t s) {
+cudaError_t flow_launch_imap(int* cells, int nf, int* imap, const Grid& g, int ys, int xs,
+                             cudaStream_t s) {
     if (nf <= 0) return cudaSuccess;
-    imap_scatter_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(cells, nf, imap);
+    imap_scatter_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(cells, nf, imap, g, ys, xs);
     return cudaGetLastError();
 }
 

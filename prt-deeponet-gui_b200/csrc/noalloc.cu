@@ -114,7 +114,8 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
     g.ny = p->nd == 3 ? p->dims[1] : 1;
     g.nz = p->nd == 3 ? p->dims[2] : p->dims[1];
     g.n = (long long)g.nx * g.ny * g.nz;
-    if (g.n >= (1ll << 31)) return fail(PRT_E_INVALID, "grid too large");
+    if (g.n >= (1ll << 31) || coord_bits(g.nx) + coord_bits(g.ny) + coord_bits(g.nz) > 32)
+        return fail(PRT_E_INVALID, "grid too large");
     const int Q = p->nd == 3 ? 19 : 9;
     const size_t es = p->precision == PRT_FP64 ? 8 : (p->precision == PRT_FP16 ? 2 : 4);
     // scratch layout, sized for the worst case (every voxel pore):
@@ -194,8 +195,10 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
     NCK(cudaStreamSynchronize(s));
     NCK(adr_launch_compact(flag, g.n, cnt, count, cells, s));
     NCK(cudaMemsetAsync(imap, 0xff, (size_t)g.n * 4, s));
-    NCK(flow_launch_imap(cells, (int)nfluid, imap, s));
     FlowMap fm;
+    fm.ys = coord_bits(g.nz);
+    fm.xs = fm.ys + coord_bits(g.ny);
+    NCK(flow_launch_imap(cells, (int)nfluid, imap, g, fm.ys, fm.xs, s));
     fm.nf = (int)nfluid;
     fm.cells = cells;
     fm.imap = imap;

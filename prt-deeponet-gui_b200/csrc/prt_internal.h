@@ -101,13 +101,31 @@ struct PairTree {
     const int* level_off;  // nlevel + 1 offsets into the inner arrays
 };
 
-// The pore-only layout of a flow solve: lattice slot k holds pore voxel
-// cells[k] (C order); imap[voxel] is the slot of a pore voxel, -1 for rock.
+// The pore-only layout of a flow solve: lattice slot k holds the k-th pore
+// voxel in C order, whose coordinates are packed in cells[k] as
+// x << xs | y << ys | z (so a kernel finds its neighbours with shifts and
+// masks instead of divisions); imap[voxel] is the slot of a pore voxel, -1
+// for rock.
 struct FlowMap {
     int nf;
     const int* cells;
     const int* imap;
+    int ys, xs;  // bit offsets of y and x in a packed cell
 };
+
+// Bits that hold the values 0 .. n-1.
+__host__ __device__ inline int coord_bits(int n) {
+    int b = 0;
+    while (b < 31 && (1 << b) < n) ++b;
+    return b;
+}
+
+__host__ __device__ inline void unpack_cell(unsigned cv, const FlowMap& fm, int& x, int& y,
+                                            int& z) {
+    z = (int)(cv & ((1u << fm.ys) - 1u));
+    y = (int)((cv >> fm.ys) & ((1u << (fm.xs - fm.ys)) - 1u));
+    x = (int)(cv >> fm.xs);
+}
 
 // Kernel launchers (lb_flow.cu) ---------------------------------------------
 // Returns cudaSuccess or the launch error.  f holds the two lattices (read /
@@ -124,7 +142,10 @@ cudaError_t flow_launch_moments(int nd, int precision, bool odd, const void* f,
                                 float* vel, double* partials, cudaStream_t s);
 cudaError_t flow_launch_flags(const uint8_t* mat, long long n, int pore, uint8_t* flag,
                               cudaStream_t s);
-cudaError_t flow_launch_imap(const int* cells, int nf, int* imap, cudaStream_t s);
+// imap[cells[k]] = k, then cells[k] rewritten from the voxel index to the
+// packed coordinates of fm (imap must hold -1 everywhere before).
+cudaError_t flow_launch_imap(int* cells, int nf, int* imap, const Grid& g, int ys, int xs,
+                             cudaStream_t s);
 cudaError_t flow_launch_final_reduce(const double* partials, int nblocks, double* out,
                                      cudaStream_t s);
 int flow_blocks(long long n);

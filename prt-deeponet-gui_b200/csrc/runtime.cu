@@ -119,8 +119,10 @@ int prt::flow_setup(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p
     const Grid g = make_grid(p->nd, p->dims);
     const int Q = p->nd == 3 ? 19 : 9;
     const size_t es = p->precision == PRT_FP64 ? 8 : (p->precision == PRT_FP16 ? 2 : 4);
-    if (g.n >= (1ll << 31))
-        return fail(ctx, PRT_E_INVALID, "grids of 2^31 voxels or more are not supported");
+    if (g.n >= (1ll << 31) || coord_bits(g.nx) + coord_bits(g.ny) + coord_bits(g.nz) > 32)
+        return fail(ctx, PRT_E_INVALID,
+                    "grids of 2^31 voxels or more (or whose packed coordinates exceed 32 bits) "
+                    "are not supported");
     // pore-only layout: flags, compacted voxel list, voxel -> slot map
     CK(F.flag.ensure((size_t)g.n));
     CK(F.cnt.ensure((size_t)((g.n + 1023) / 1024) * 4));
@@ -136,7 +138,10 @@ int prt::flow_setup(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p
     CK(adr_launch_compact(F.flag.as<uint8_t>(), g.n, F.cnt.as<int>(), F.count.as<long long>(),
                           F.cells.as<int>(), s));
     CK(cudaMemsetAsync(F.fluid.p, 0xff, (size_t)g.n * 4, s));
-    CK(flow_launch_imap(F.cells.as<int>(), (int)nfluid, F.fluid.as<int>(), s));
+    F.fm.ys = coord_bits(g.nz);
+    F.fm.xs = F.fm.ys + coord_bits(g.ny);
+    CK(flow_launch_imap(F.cells.as<int>(), (int)nfluid, F.fluid.as<int>(), g, F.fm.ys, F.fm.xs,
+                        s));
     ctx->launches += 7;
     F.fm.nf = (int)nfluid;
     F.fm.cells = F.cells.as<int>();
