@@ -32,13 +32,18 @@ Multi-GPU: replicas only (the path does not shard; one independent solve per
 rank), value = all ranks' updates / max-over-ranks time.
 """
 
-import argparse
-import contextlib
+import os
+
+# concurrent solves need more than the default 8 hardware work queues; read
+# when the CUDA context is created, so before torch touches the device
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
+import argparse  # noqa: E402
+import contextlib  # noqa: E402
 import ctypes
 import io
 import json
 import multiprocessing as mp
-import os
 import statistics
 import subprocess
 import sys
@@ -320,9 +325,13 @@ def run_batched(args, torch):
     torch.cuda.synchronize()
     with Clocks(0) as clk:
         t0 = time.perf_counter()
-        res = solve_batch(reqs, quiet=True)
+        res = solve_batch(reqs, quiet=True, mode="streams")
         torch.cuda.synchronize()
         t_batch = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        res_tiles = solve_batch(reqs, quiet=True, mode="tiles")
+        torch.cuda.synchronize()
+        t_tiles = time.perf_counter() - t0
         t0 = time.perf_counter()
         ref = [plain_solve(r, ctx) for r in reqs]
         torch.cuda.synchronize()
@@ -340,7 +349,11 @@ def run_batched(args, torch):
                                    "order / reversible sorption, D3Q19 fp32 to tol 1e-6 (cap "
                                    "30000) + ADR to the stop rule (cap 100000)" % n,
                        "voxels": cells, "seed": SEED, "geometry_s": round(gen_s, 2)},
+            "mode": "streams: every solve's flow and transport loops as CUDA graphs on its own "
+                    "stream, all solves at once",
             "plain": {"solves_per_hour": n / t_plain * 3600.0, "seconds": t_plain},
+            "tiles": {"solves_per_hour": n / t_tiles * 3600.0, "seconds": t_tiles,
+                      "identical_to_plain": all(_same(a, b) for a, b in zip(res_tiles, ref))},
             "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": same,
             "failed": sum(1 for r in res if r.error is not None), "clocks": clk.summary()}
 
@@ -364,7 +377,7 @@ def run_served(args, torch):
         solve_batch(small, quiet=True)
     torch.cuda.synchronize()
     with Clocks(0) as clk:
-        srv = serve(reqs, arrivals)
+        srv = serve(reqs, arrivals, mode=args.serve_mode)
         torch.cuda.synchronize()
         # plain: one server, first come first served, same arrival times
         t0 = time.perf_counter()
@@ -386,7 +399,8 @@ def run_served(args, torch):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "served: %d requests, Poisson %.3g req/s, edge U{32..160}, "
-                                   "draws as the batched set, 80%% HBM admission" % (n, args.rate),
+                                   "draws as the batched set, 80%% HBM admission, %s" % (
+                                       n, args.rate, args.serve_mode),
                        "seed": SEED, "geometry_s": round(gen_s, 2)},
             "latency_p50_s": S["latency_p50_s"], "latency_p99_s": S["latency_p99_s"],
             "queue_p50_s": S["queue_p50_s"], "completed": S["completed"], "failed": S["failed"],
@@ -454,6 +468,7 @@ def main():
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"])
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--serve-mode", default="streams", choices=["streams", "tiles"])
     args = ap.parse_args()
     if args.mode != "plain" and args.impl == "ours":
         import torch

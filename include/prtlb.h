@@ -309,6 +309,16 @@ int prt_adr_start(prt_ctx* ctx, const prt_adr_run_params* rp);
  * prt_adr_ladder / prt_adr_fetch work as after prt_adr_run. */
 int prt_adr_finish(prt_ctx* ctx, prt_adr_result* res);
 
+/* Concurrent solves: enqueue the whole flow loop of a started solve
+ * (prt_flow_start), or the whole transport loop of a started run
+ * (prt_adr_start), on the context's own stream and return at once; many
+ * contexts then run side by side on one GPU, each loop as one CUDA graph.
+ * prt_ctx_busy reports whether the enqueued loop is still running; the
+ * results are read with prt_flow_finish / prt_adr_finish (which wait). */
+int prt_flow_launch(prt_ctx* ctx);
+int prt_adr_launch(prt_ctx* ctx);
+int prt_ctx_busy(prt_ctx* ctx, int32_t* busy);
+
 typedef struct prt_batch prt_batch;
 
 /* A batch on CUDA device `device`, with its own stream.  Each step advances
@@ -348,8 +358,10 @@ int prt_batch_collect(prt_batch* b, prt_ctx** out, int32_t cap, int32_t* count);
 /* Jobs in the batch (pending additions included). */
 int prt_batch_size(const prt_batch* b, int32_t* flow_jobs, int32_t* adr_jobs);
 
-/* Tile size in 256-voxel blocks (1, 2 or 4) and persistent grid multiple
- * (1 or 2 resident waves); 0, 0 = choose by timing the first launches. */
+/* Tile size in 256-voxel blocks (1, 2 or 4) and grid: a persistent grid of
+ * grid_mult (1 or 2) resident waves walking the work list, or 0 for one
+ * block per work-list entry; tile_blocks 0 = choose both by timing the
+ * first launches. */
 int prt_batch_tune(prt_batch* b, int32_t tile_blocks, int32_t grid_mult);
 
 /* out8: kernel launches, graph builds, tile blocks, grid multiple, steps

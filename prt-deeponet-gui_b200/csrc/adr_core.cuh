@@ -44,14 +44,25 @@ struct VoxelPos {
     long long c;
 };
 
+// Coordinates of voxel c (grids hold fewer than 2^31 voxels, so 32-bit
+// division is exact).
 __device__ __forceinline__ VoxelPos voxel_pos(long long c, const Grid& g) {
     VoxelPos v;
     v.c = c;
-    unsigned long long t = (unsigned long long)c;
+    unsigned t = (unsigned)c;
     v.p[2] = (int)(t % (unsigned)g.nz);
     t /= (unsigned)g.nz;
     v.p[1] = (int)(t % (unsigned)g.ny);
     v.p[0] = (int)(t / (unsigned)g.ny);
+    return v;
+}
+
+// A load that is always issued, before the flags that decide whether its
+// value is used are known: the address is in bounds either way (an
+// edge-clamped neighbour), and the buffer is not written by this launch.
+__device__ __forceinline__ float ld_early(const float* p) {
+    float v;
+    asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
     return v;
 }
 
@@ -77,7 +88,8 @@ __device__ __forceinline__ long long face_step(const Grid& g, int a) {
 // value (step(), prtlb_3d.py:1392-1400, pins before transport).
 __device__ __forceinline__ float ld_c(const float* __restrict__ Cj, long long c, int x, bool pin,
                                       float feed) {
-    return (pin && x == 0) ? feed : Cj[c];
+    const float v = ld_early(Cj + c);
+    return (pin && x == 0) ? feed : v;
 }
 
 // transport() of one chemical at one voxel (prtlb_3d.py:1182-1208).
@@ -102,13 +114,19 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
         const int x0 = v.p[0];
         const int xm1 = (a == 0) ? pm1 : x0, xm2 = (a == 0) ? pm2 : x0;
         const int xp1 = (a == 0) ? pp1 : x0, xp2 = (a == 0) ? pp2 : x0;
-        const float Cm1 = oL ? ld_c(Cj, v.c + (long long)(pm1 - p) * s, xm1, pin, feed) : Cc;
-        const float Cp1 = oH ? ld_c(Cj, v.c + (long long)(pp1 - p) * s, xp1, pin, feed) : Cc;
-        const float Cm2 = fL ? ld_c(Cj, v.c + (long long)(pm2 - p) * s, xm2, pin, feed) : Cm1;
-        const float Cp2 = fH ? ld_c(Cj, v.c + (long long)(pp2 - p) * s, xp2, pin, feed) : Cp1;
+        // all four neighbours and both faces are loaded before the flags
+        // choose among them (clamped addresses are always in the grid)
+        const float vm1 = ld_c(Cj, v.c + (long long)(pm1 - p) * s, xm1, pin, feed);
+        const float vp1 = ld_c(Cj, v.c + (long long)(pp1 - p) * s, xp1, pin, feed);
+        const float vm2 = ld_c(Cj, v.c + (long long)(pm2 - p) * s, xm2, pin, feed);
+        const float vp2 = ld_c(Cj, v.c + (long long)(pp2 - p) * s, xp2, pin, feed);
         const long long fi = face_lo(g, v, a);
-        const float uL = face[a][fi];
-        const float uH = face[a][fi + face_step(g, a)];
+        const float uL = ld_early(face[a] + fi);
+        const float uH = ld_early(face[a] + fi + face_step(g, a));
+        const float Cm1 = oL ? vm1 : Cc;
+        const float Cp1 = oH ? vp1 : Cc;
+        const float Cm2 = fL ? vm2 : Cm1;
+        const float Cp2 = fH ? vp2 : Cp1;
         const int bf = (fl & F_BF) ? 1 : 0;
         // face diffusivity by the biofilm count of its two voxels (0, 1, 2);
         // selected, not indexed, so the table stays in registers

@@ -25,18 +25,22 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
                       const int* __restrict__ ntiles_p) {
     using S = typename M::S;
     __shared__ int s_last;
-    __shared__ FlowJob sj;  // the tile's job: constants read where they are used
-    const int ntiles = *ntiles_p;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    __shared__ __align__(16) FlowJob sj;  // the tile's job: constants read where they are used
+    int t0, t1, cur = -1;
+    tile_range(*ntiles_p, t0, t1);
+    for (int t = t0; t < t1; ++t) {
         const BatchTile tl = tiles[t];
-        if (threadIdx.x == 0) sj = jobs[tl.job];
+        if (tl.job != cur) {  // uniform over the block
+            block_copy(&sj, jobs + tl.job);
+            cur = tl.job;
+        }
         __syncthreads();
         FlowCtrl* ctrl = sj.ctrl;
         const long long it = __ldcg(&ctrl->it_base);
         const bool run = !__ldcg(&ctrl->done) && it < __ldcg(&ctrl->nit);
         const bool check = __ldcg(&ctrl->tol) > 0 && ((it + 1) % __ldcg(&ctrl->every)) == 0;
         if (!run) {  // uniform over the block
-            __syncthreads();  // sj is rewritten by the next tile
+            __syncthreads();  // every thread has read ctrl before sj may change
             continue;
         }
         const int nf = sj.fm.nf;

@@ -19,10 +19,19 @@ template <int ND, int NS>
 __global__ void __launch_bounds__(kBatchAdrThreads)
     batch_adr_kernel(const AdrJob* __restrict__ jobs, const BatchTile* __restrict__ tiles,
                      const int* __restrict__ ntiles_p) {
-    const int ntiles = *ntiles_p;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    // the tile's job in shared memory: the per-voxel code reads its many
+    // constants (feeds, diffusivities, rate constants) from there
+    __shared__ __align__(16) AdrJob J;
+    int t0, t1, cur = -1;
+    tile_range(*ntiles_p, t0, t1);
+    for (int t = t0; t < t1; ++t) {
         const BatchTile tl = tiles[t];
-        const AdrJob& J = jobs[tl.job];
+        if (tl.job != cur) {  // uniform over the block
+            __syncthreads();  // the previous job's voxels are done with J
+            block_copy(&J, jobs + tl.job);
+            __syncthreads();
+            cur = tl.job;
+        }
         const AdrCtrl* ctrl = J.ctrl;
         if (ctrl->done) continue;
         const long long n = ctrl->n_base + 1;

@@ -46,7 +46,8 @@ struct Candidate {
     int tile_blocks;
     int grid_mult;
 };
-const Candidate kCandidates[] = {{1, 1}, {2, 1}, {4, 1}, {1, 2}};
+// grid_mult 0: one block per work-list entry (no persistent loop)
+const Candidate kCandidates[] = {{1, 0}, {1, 1}, {2, 1}, {4, 0}};
 constexpr int kNumCandidates = 4;
 
 }  // namespace
@@ -219,7 +220,8 @@ int rebuild(prt_batch* b) {
         int occ = 1;
         if (c < kFlowClasses) occ = batch_flow_occupancy(c >= 4 ? 3 : 2, c % 4);
         else occ = batch_adr_occupancy(c >= kFlowClasses + 8 ? 3 : 2, (c - kFlowClasses) % 8 + 1);
-        b->grid[c] = std::max(1, std::min(nt, b->grid_mult * occ * b->nsm));
+        b->grid[c] = b->grid_mult == 0 ? nt
+                                       : std::max(1, std::min(nt, b->grid_mult * occ * b->nsm));
     }
     b->grid[kClasses] = std::max(1, std::min((int)b->h_leaf.size(), 4 * b->nsm));
     b->grid[kClasses + 1] = std::max(1, std::min(b->nadr, 2 * b->nsm));
@@ -344,6 +346,12 @@ extern "C" int prt_flow_finish(prt_ctx* ctx, float* vel_out, prt_flow_info* info
     if (ctx->batch) return fail(ctx, PRT_E_STATE, "the context is in a batch");
     if (!ctx->flow_armed) return fail(ctx, PRT_E_STATE, "no started flow solve");
     CK(cudaSetDevice(ctx->device));
+    if (ctx->running) {
+        int32_t busy = 0;
+        CK(cudaEventSynchronize(ctx->ev[1]));
+        int rc0 = prt_ctx_busy(ctx, &busy);
+        if (rc0 != PRT_OK) return rc0;
+    }
     FlowState& F = ctx->flow;
     FlowCtrl res;
     CK(cudaMemcpyAsync(&res, F.ctrl.p, sizeof(res), cudaMemcpyDeviceToHost, ctx->stream));
@@ -399,6 +407,12 @@ extern "C" int prt_adr_finish(prt_ctx* ctx, prt_adr_result* res) {
     if (ctx->batch) return fail(ctx, PRT_E_STATE, "the context is in a batch");
     if (!ctx->adr_armed) return fail(ctx, PRT_E_STATE, "no started transport run");
     CK(cudaSetDevice(ctx->device));
+    if (ctx->running) {
+        int32_t busy = 0;
+        CK(cudaEventSynchronize(ctx->ev[3]));
+        int rc0 = prt_ctx_busy(ctx, &busy);
+        if (rc0 != PRT_OK) return rc0;
+    }
     AdrCtrl cur;
     CK(cudaMemcpyAsync(&cur, ctx->adr.ctrl.p, sizeof(cur), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -407,6 +421,53 @@ extern "C" int prt_adr_finish(prt_ctx* ctx, prt_adr_result* res) {
     if (rc != PRT_OK) return rc;
     ctx->adr_armed = false;
     ctx->timing[3] = (double)cur.n_base;
+    return PRT_OK;
+}
+
+// ===========================================================================
+// concurrent solves: each loop enqueued on its context's own stream
+// ===========================================================================
+extern "C" int prt_flow_launch(prt_ctx* ctx) {
+    if (!ctx) return PRT_E_INVALID;
+    if (ctx->batch) return fail(ctx, PRT_E_STATE, "the context is in a batch");
+    if (!ctx->flow_armed) return fail(ctx, PRT_E_STATE, "no started flow solve");
+    if (ctx->running) return fail(ctx, PRT_E_STATE, "a loop is already running on this context");
+    CK(cudaSetDevice(ctx->device));
+    int rc = flow_loop_async(ctx);
+    if (rc != PRT_OK) return rc;
+    ctx->running = 1;
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_launch(prt_ctx* ctx) {
+    if (!ctx) return PRT_E_INVALID;
+    if (ctx->batch) return fail(ctx, PRT_E_STATE, "the context is in a batch");
+    if (!ctx->adr_armed) return fail(ctx, PRT_E_STATE, "no started transport run");
+    if (ctx->running) return fail(ctx, PRT_E_STATE, "a loop is already running on this context");
+    CK(cudaSetDevice(ctx->device));
+    int rc = adr_loop_async(ctx);
+    if (rc != PRT_OK) return rc;
+    ctx->running = 2;
+    return PRT_OK;
+}
+
+extern "C" int prt_ctx_busy(prt_ctx* ctx, int32_t* busy) {
+    if (!ctx || !busy) return PRT_E_INVALID;
+    *busy = 0;
+    if (!ctx->running) return PRT_OK;
+    CK(cudaSetDevice(ctx->device));
+    cudaEvent_t a = ctx->running == 1 ? ctx->ev[0] : ctx->ev[2];
+    cudaEvent_t b = ctx->running == 1 ? ctx->ev[1] : ctx->ev[3];
+    const cudaError_t e = cudaEventQuery(b);
+    if (e == cudaErrorNotReady) {
+        *busy = 1;
+        return PRT_OK;
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaEventQuery");
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    ctx->timing[ctx->running == 1 ? 0 : 2] = ms;
+    ctx->running = 0;
     return PRT_OK;
 }
 
@@ -477,6 +538,7 @@ extern "C" int prt_batch_add(prt_batch* b, prt_ctx* job) {
     if (job->device != b->device) return bfail(b, PRT_E_INVALID, "the context is on another device");
     if (!job->flow_armed && !job->adr_armed)
         return bfail(b, PRT_E_STATE, "the context has no started flow solve or transport run");
+    if (job->running) return bfail(b, PRT_E_STATE, "the context's loop is running on its stream");
     std::lock_guard<std::mutex> lk(b->mu);
     b->jobs.push_back(job);
     job->batch = b;
@@ -622,14 +684,15 @@ extern "C" int prt_batch_size(const prt_batch* b, int32_t* flow_jobs, int32_t* a
 extern "C" int prt_batch_tune(prt_batch* b, int32_t tile_blocks, int32_t grid_mult) {
     if (!b) return PRT_E_INVALID;
     std::lock_guard<std::mutex> lk(b->mu);
-    if (tile_blocks == 0 && grid_mult == 0) {
+    if (tile_blocks == 0) {
         b->tuning = true;
         b->cand = 0;
         return PRT_OK;
     }
     if (!(tile_blocks == 1 || tile_blocks == 2 || tile_blocks == 4) ||
-        !(grid_mult == 1 || grid_mult == 2))
-        return bfail(b, PRT_E_INVALID, "tile blocks must be 1, 2 or 4 and the grid multiple 1 or 2");
+        !(grid_mult == 0 || grid_mult == 1 || grid_mult == 2))
+        return bfail(b, PRT_E_INVALID,
+                     "tile blocks must be 1, 2 or 4 and the grid multiple 0, 1 or 2");
     b->tuning = false;
     if (tile_blocks != b->tile_blocks || grid_mult != b->grid_mult) b->dirty = true;
     b->tile_blocks = tile_blocks;

@@ -226,6 +226,24 @@ struct LeafItem {
     int pad;
 };
 
+// Copy of a job descriptor into shared memory by the whole block (8-byte
+// words), so per-voxel code reads its constants from shared memory.
+template <class T>
+__device__ __forceinline__ void block_copy(T* dst, const T* src) {
+    static_assert(sizeof(T) % 8 == 0, "descriptor size must be a multiple of 8 bytes");
+    const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(T) / 8); i += blockDim.x) d[i] = s[i];
+}
+
+// The contiguous range of work-list entries block b of g handles, so that
+// consecutive tiles of a block mostly belong to one job.
+__device__ __forceinline__ void tile_range(int n, int& t0, int& t1) {
+    const long long b = blockIdx.x, g = gridDim.x;
+    t0 = (int)(b * n / g);
+    t1 = (int)((b + 1) * n / g);
+}
+
 // Each launch is persistent: `grid` blocks walk the work list, whose length
 // is read on the device so a captured graph stays valid when the list is
 // rewritten between replays.

@@ -218,49 +218,82 @@ int prt::flow_finish(prt_ctx* ctx, prt_flow_info* info) {
     return PRT_OK;
 }
 
+// The flow loop's graph body: `every` step kernels and the convergence
+// check (which sets the WHILE condition when h is used).
+static cudaError_t flow_emit(prt_ctx* ctx, cudaGraphConditionalHandle h, int use) {
+    FlowState& F = ctx->flow;
+    const prt_flow_params& p = F.p;
+    FlowCtrl* dctrl = F.ctrl.as<FlowCtrl>();
+    double* parts = F.partials.as<double>();
+    for (int k = 0; k < p.every; ++k) {
+        cudaError_t e = flow_launch_step(p.nd, p.precision, (k & 1) != 0, k == p.every - 1,
+                                         F.f.p, F.fm, F.g, F.kc, dctrl, k, parts, ctx->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return flow_launch_check(dctrl, parts, F.nb, h, use, ctx->stream);
+}
+
+// Builds the loop graph of the set-up flow solve, or reuses the cached one
+// when nothing it bakes in has changed.
+static int flow_graph(prt_ctx* ctx) {
+    FlowState& F = ctx->flow;
+    const prt_flow_params& p = F.p;
+    FlowKey key;
+    key.nd = p.nd; key.precision = p.precision; key.every = p.every; key.g = F.g;
+    key.force = p.force; key.tau = p.tau; key.magic = p.magic; key.nit = p.nit;
+    key.tol = p.tol; key.f = F.f.p;
+    key.aux[0] = F.fluid.p; key.aux[1] = F.partials.p; key.aux[2] = F.ctrl.p;
+    key.aux[3] = F.cells.p; key.nf = F.nfluid;
+    if (!F.graph.exec || !(key == F.key)) {
+        CK(build_while_graph(ctx->stream,
+                             F.graph, [&](cudaGraphConditionalHandle h, int use) {
+                                 return flow_emit(ctx, h, use);
+                             }));
+        F.key = key;
+    }
+    return PRT_OK;
+}
+
+// Enqueues the whole flow loop of the set-up solve on the context's stream
+// without waiting (ev[0] / ev[1] bracket it): one launch of the WHILE graph,
+// or every chunk of the plain graph where conditional nodes are missing
+// (chunks after the stop are no-ops).
+int prt::flow_loop_async(prt_ctx* ctx) {
+    FlowState& F = ctx->flow;
+    cudaStream_t s = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[0], s));
+    if (F.p.nit > 0) {
+        int rc = flow_graph(ctx);
+        if (rc != PRT_OK) return rc;
+        const long long chunks = F.graph.conditional ? 1 : (F.p.nit + F.p.every - 1) / F.p.every;
+        for (long long r = 0; r < chunks; ++r) CK(cudaGraphLaunch(F.graph.exec, s));
+    }
+    CK(cudaEventRecord(ctx->ev[1], s));
+    return PRT_OK;
+}
+
 extern "C" int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p,
                             float* d_vel, prt_flow_info* info) {
     int rc = flow_setup(ctx, d_mat, p, d_vel);
     if (rc != PRT_OK) return rc;
     FlowState& F = ctx->flow;
     cudaStream_t s = ctx->stream;
-    const Grid g = F.g;
-    const FlowMap fm = F.fm;
-    const LbParams kc = F.kc;
-    const int nb = F.nb;
     FlowCtrl* dctrl = F.ctrl.as<FlowCtrl>();
-    double* parts = F.partials.as<double>();
     const int every = p->every;
-    auto emit = [&](cudaGraphConditionalHandle h, int use) -> cudaError_t {
-        for (int k = 0; k < every; ++k) {
-            cudaError_t e = flow_launch_step(p->nd, p->precision, (k & 1) != 0, k == every - 1,
-                                             F.f.p, fm, g, kc, dctrl, k, parts, s);
-            if (e != cudaSuccess) return e;
-        }
-        return flow_launch_check(dctrl, parts, nb, h, use, s);
-    };
     CK(cudaEventRecord(ctx->ev[0], s));
     if (p->nit > 0) {
         if (graphs_disabled()) {
             // direct launches, chunk by chunk
             FlowCtrl hc2{};
             while (!hc2.done) {
-                CK(emit(cudaGraphConditionalHandle(0), 0));
+                CK(flow_emit(ctx, cudaGraphConditionalHandle(0), 0));
                 ctx->launches += every + 1;
                 CK(cudaMemcpyAsync(&hc2, dctrl, sizeof(hc2), cudaMemcpyDeviceToHost, s));
                 CK(cudaStreamSynchronize(s));
             }
         } else {
-            FlowKey key;
-            key.nd = p->nd; key.precision = p->precision; key.every = every; key.g = g;
-            key.force = p->force; key.tau = p->tau; key.magic = p->magic; key.nit = p->nit;
-            key.tol = p->tol; key.f = F.f.p;
-            key.aux[0] = F.fluid.p; key.aux[1] = F.partials.p; key.aux[2] = F.ctrl.p;
-            key.aux[3] = F.cells.p; key.nf = F.nfluid;
-            if (!F.graph.exec || !(key == F.key)) {
-                CK(build_while_graph(s, F.graph, emit));
-                F.key = key;
-            }
+            rc = flow_graph(ctx);
+            if (rc != PRT_OK) return rc;
             const long long chunks = (p->nit + every - 1) / every;
             if (F.graph.conditional) {
                 CK(cudaGraphLaunch(F.graph.exec, s));
@@ -618,6 +651,41 @@ int prt::adr_run_finish(prt_ctx* ctx, prt_adr_result* res) {
     return PRT_OK;
 }
 
+// The transport loop's graph body: `check` step kernels, the numpy-order
+// means of the chunk's last step and the stop rule (which sets the WHILE
+// condition when h is used).
+static cudaError_t adr_emit(prt_ctx* ctx, cudaGraphConditionalHandle h, int use) {
+    AdrState& A = ctx->adr;
+    AdrCtrl* dctrl = A.ctrl.as<AdrCtrl>();
+    float* dmeans = A.means.as<float>();
+    const float** srcp = (const float**)A.src_slot.p;
+    for (int k = 0; k < A.rp.check; ++k) {
+        cudaError_t e = adr_launch_step(A.d, A.p, dctrl, k, ctx->stream);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = adr_launch_chunk_means(A.d, dctrl, srcp, dmeans, ctx->stream);
+    if (e != cudaSuccess) return e;
+    return adr_launch_stop(A.d, dctrl, dmeans, h, use, ctx->stream);
+}
+
+// Enqueues the whole transport loop of a started run (adr_run_setup with no
+// pause) without waiting (ev[2] / ev[3] bracket it), as flow_loop_async.
+int prt::adr_loop_async(prt_ctx* ctx) {
+    AdrState& A = ctx->adr;
+    cudaStream_t s = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[2], s));
+    if (A.rp.limit > 0) {
+        CK(build_while_graph(s, A.graph, [&](cudaGraphConditionalHandle h, int use) {
+            return adr_emit(ctx, h, use);
+        }));
+        const long long chunks =
+            A.graph.conditional ? 1 : (A.rp.limit + A.rp.check - 1) / A.rp.check;
+        for (long long r = 0; r < chunks; ++r) CK(cudaGraphLaunch(A.graph.exec, s));
+    }
+    CK(cudaEventRecord(ctx->ev[3], s));
+    return PRT_OK;
+}
+
 extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progress_cb cb,
                            void* user, prt_adr_result* res) {
     if (!ctx || !rp) return fail(ctx, PRT_E_INVALID, "null argument");
@@ -631,18 +699,9 @@ extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progr
     const int log_cap = A.d.log_cap;
     AdrCtrl* dctrl = A.ctrl.as<AdrCtrl>();
     const int check = rp->check;
-    const prt_adr_params P = A.p;
     const AdrDev D = A.d;
-    float* dmeans = A.means.as<float>();
-    const float** srcp = (const float**)A.src_slot.p;
     auto emit = [&](cudaGraphConditionalHandle h, int use) -> cudaError_t {
-        for (int k = 0; k < check; ++k) {
-            cudaError_t e = adr_launch_step(D, P, dctrl, k, s);
-            if (e != cudaSuccess) return e;
-        }
-        cudaError_t e = adr_launch_chunk_means(D, dctrl, srcp, dmeans, s);
-        if (e != cudaSuccess) return e;
-        return adr_launch_stop(D, dctrl, dmeans, h, use, s);
+        return adr_emit(ctx, h, use);
     };
     const int per_chunk = check + 3 + (D.tree.nleaf > 0 ? 1 : 0);
     std::vector<ProgressRec> logbuf;

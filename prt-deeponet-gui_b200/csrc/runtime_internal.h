@@ -142,6 +142,7 @@ struct prt_ctx {
     bool flow_armed = false;  // flow set up, its time loop not finished
     bool adr_armed = false;   // transport run set up, its time loop not finished
     prt_batch* batch = nullptr;  // the batch holding this context, if any
+    int running = 0;             // a loop enqueued by prt_*_launch: 1 flow, 2 transport
 };
 
 namespace prt {
@@ -273,6 +274,10 @@ int flow_setup(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p, flo
 int flow_finish(prt_ctx* ctx, prt_flow_info* info);
 int adr_run_setup(prt_ctx* ctx, const prt_adr_run_params* rp, long long pause_every);
 int adr_run_finish(prt_ctx* ctx, prt_adr_result* res);
+// Enqueue the whole flow / transport loop of a started solve on the
+// context's stream without waiting (runtime.cu).
+int flow_loop_async(prt_ctx* ctx);
+int adr_loop_async(prt_ctx* ctx);
 // Takes ctx out of its batch (engine.cu); used by prt_destroy.
 void batch_detach(prt_ctx* ctx);
 

@@ -9,6 +9,10 @@ import ctypes
 import os
 import threading
 
+# concurrent solves (one stream each) need more than the default 8 hardware
+# work queues; read when the process creates its CUDA context
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libprtlb.so")
 
@@ -120,6 +124,9 @@ _PROTOS = {
     "prt_flow_release": (ctypes.c_int, [ctypes.c_void_p]),
     "prt_adr_start": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdrRunParams)]),
     "prt_adr_finish": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(AdrResult)]),
+    "prt_flow_launch": (ctypes.c_int, [ctypes.c_void_p]),
+    "prt_adr_launch": (ctypes.c_int, [ctypes.c_void_p]),
+    "prt_ctx_busy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(c_i32)]),
     "prt_batch_create": (ctypes.c_int, [ctypes.c_int, c_i32, ctypes.POINTER(ctypes.c_void_p)]),
     "prt_batch_destroy": (None, [ctypes.c_void_p]),
     "prt_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),

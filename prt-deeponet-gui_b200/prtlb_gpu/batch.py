@@ -154,8 +154,10 @@ class Batch(object):
         return {k: float(out[i]) for i, k in enumerate(keys)}
 
     def tune(self, tile_blocks=0, grid_mult=0):
-        """Fix the tiling (tile_blocks 1/2/4, grid_mult 1/2) or, with 0, 0,
-        let the next launches time the candidates and keep the fastest."""
+        """Fix the tiling (tile_blocks 1/2/4; grid_mult 1/2 resident waves of
+        persistent blocks, or 0 for one block per tile) or, with
+        tile_blocks 0, let the next launches time the candidates and keep
+        the fastest."""
         self._check(_lib.lib().prt_batch_tune(self.handle, int(tile_blocks), int(grid_mult)))
 
     def _quiet(self):
@@ -178,13 +180,17 @@ class Batch(object):
             L = _lib.lib()
             ctx.check(L.prt_flow_start(ctx.handle, g.ctypes.data_as(ctypes.c_void_p),
                                        ctypes.byref(p)))
-            self._check(L.prt_batch_add(self.handle, ctx.handle))
+            self._enqueue(ctx, "flow")
         except BaseException:
             ctx.close()
             raise
         job = _Job(req, ctx, res)
         self._jobs[ctx.handle.value] = job
         return res
+
+    def _enqueue(self, ctx, phase):
+        """A started solve (its flow or its transport loop) joins the batch."""
+        self._check(_lib.lib().prt_batch_add(self.handle, ctx.handle))
 
     def launch(self, steps=None):
         """Enqueue `steps` batch steps (default: one graph replay)."""
@@ -302,7 +308,7 @@ class Batch(object):
         ctx.check(L.prt_flow_release(ctx.handle))
         R = _adr.run_params(S, a["steps"], a["tol"], a["max_steps"], a["ratio"])
         ctx.check(L.prt_adr_start(ctx.handle, ctypes.byref(R)))
-        self._check(L.prt_batch_add(self.handle, ctx.handle))
+        self._enqueue(ctx, "adr")
         job.phase = "adr"
 
     def _adr_done(self, job):
@@ -327,6 +333,81 @@ class Batch(object):
         job.phase = "done"
 
 
+class StreamBatch(Batch):
+    """The same interface over concurrent single-solve loops: every solve
+    runs its own flow loop, then its own transport loop, each as one CUDA
+    graph launched on the solve's own stream (prt_flow_launch /
+    prt_adr_launch), so many solves share the GPU at once and each keeps the
+    single-solve kernels.  wait() returns when at least one solve finished
+    its current loop (or after `poll_s` with nothing finished)."""
+
+    def __init__(self, device=0, quiet=False, poll_s=0.002):
+        self.handle = None
+        self.device = int(device)
+        self.graph_steps = 0
+        self.quiet = bool(quiet)
+        self.poll_s = float(poll_s)
+        self._jobs = {}
+        self._ready = []
+        self._graveyard = []
+        self._in_flight = False
+        self.finished = []
+        self._launches = 0
+
+    def _check(self, rc):
+        if rc != _lib.PRT_OK:
+            raise _lib.PrtError(rc, "stream batch call failed")
+
+    def close(self):
+        for job in list(self._jobs.values()):
+            job.ctx.close()
+        self._jobs.clear()
+        self._ready = []
+        self._bury()
+
+    def stats(self):
+        return {"launches": float(self._launches), "graph_builds": 0.0, "tile_blocks": 0.0,
+                "grid_mult": 0.0, "steps": 0.0, "last_ms": 0.0, "tiles": 0.0}
+
+    def tune(self, tile_blocks=0, grid_mult=0):
+        pass
+
+    def _enqueue(self, ctx, phase):
+        L = _lib.lib()
+        launch = L.prt_flow_launch if phase == "flow" else L.prt_adr_launch
+        ctx.check(launch(ctx.handle))
+        self._launches += 1
+
+    def launch(self, steps=None):
+        self._in_flight = True
+
+    def wait(self, process=True):
+        L = _lib.lib()
+        busy = ctypes.c_int32()
+        t0 = time.perf_counter()
+        while True:
+            found = False
+            for key, job in list(self._jobs.items()):
+                if job in self._ready or job.phase == "done":
+                    continue
+                job.ctx.check(L.prt_ctx_busy(job.ctx.handle, ctypes.byref(busy)))
+                if not busy.value:
+                    self._ready.append(job)
+                    found = True
+            if found or not self._jobs or time.perf_counter() - t0 >= self.poll_s:
+                break
+            time.sleep(0.0002)
+        self._in_flight = False
+        self._bury()
+        return self.process() if process else []
+
+    def run(self, max_steps=None):
+        out = []
+        while self._jobs:
+            out.extend(self.advance())
+        return out
+
+
 def _needs_host_stage(req):
     """A biofilm material code makes the transport grid differ from the
     flow's pore/solid grid, so the transport is staged from the host."""
@@ -334,9 +415,12 @@ def _needs_host_stage(req):
     return chem is not None and getattr(chem, "biofilm_code", None) is not None
 
 
-def solve_batch(requests, device=0, graph_steps=20, quiet=False):
-    """Solve every Request in one batch; Results in request order."""
-    b = Batch(device=device, graph_steps=graph_steps, quiet=quiet)
+def solve_batch(requests, device=0, graph_steps=20, quiet=False, mode="tiles"):
+    """Solve every Request in one batch; Results in request order.  mode
+    "tiles": the batch engine's persistent tile-list kernels; "streams":
+    concurrent single-solve loops (StreamBatch)."""
+    b = (StreamBatch(device=device, quiet=quiet) if mode == "streams"
+         else Batch(device=device, graph_steps=graph_steps, quiet=quiet))
     try:
         results = [b.submit(r) for r in requests]
         b.run()

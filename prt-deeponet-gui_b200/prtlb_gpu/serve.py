@@ -20,7 +20,7 @@ import time
 import numpy as np
 
 from . import _lib
-from .batch import Batch, Result
+from .batch import Batch, Result, StreamBatch
 
 
 def ladder_slots(limit, ratio):
@@ -95,17 +95,20 @@ class Served(object):
 
 
 def serve(requests, arrivals, device=0, hbm_fraction=0.8, graph_steps=20, quiet=True,
-          budget_bytes=None):
+          budget_bytes=None, mode="streams"):
     """Serve `requests` arriving at host times `arrivals` (seconds after the
     start).  Admission is first-come first-served while the summed
     footprints stay within hbm_fraction of the device memory (or
-    `budget_bytes`).  Returns a Served."""
+    `budget_bytes`).  mode "streams" runs the admitted solves as concurrent
+    single-solve loops (StreamBatch), "tiles" through the batch engine's
+    tile-list kernels (Batch).  Returns a Served."""
     order = np.argsort(np.asarray(arrivals, np.float64), kind="stable")
     pending = collections.deque((float(arrivals[i]), requests[i]) for i in order)
     if budget_bytes is None:
         _, total = device_memory(device)
         budget_bytes = int(hbm_fraction * total)
-    b = Batch(device=device, graph_steps=graph_steps, quiet=quiet)
+    b = (StreamBatch(device=device, quiet=quiet) if mode == "streams"
+         else Batch(device=device, graph_steps=graph_steps, quiet=quiet))
     waiting = collections.deque()
     reserved = {}
     used = 0

@@ -96,9 +96,9 @@ def singles():
     return reqs, [_single(r) for r in reqs]
 
 
-def _batch(reqs, graph_steps=20, tiling=None, stagger=0):
-    from prtlb_gpu.batch import Batch
-    b = Batch(graph_steps=graph_steps, quiet=True)
+def _batch(reqs, graph_steps=20, tiling=None, stagger=0, mode="tiles"):
+    from prtlb_gpu.batch import Batch, StreamBatch
+    b = StreamBatch(quiet=True) if mode == "streams" else Batch(graph_steps=graph_steps, quiet=True)
     try:
         if tiling:
             b.tune(*tiling)
@@ -121,7 +121,7 @@ def test_batch_equals_single_solves(singles):
     assert st["launches"] > 0
 
 
-@pytest.mark.parametrize("tiling", [(1, 1), (2, 1), (4, 1), (1, 2)])
+@pytest.mark.parametrize("tiling", [(1, 0), (1, 1), (2, 1), (4, 0), (1, 2)])
 def test_every_tiling_gives_the_same_results(singles, tiling):
     reqs, refs = singles
     res, st = _batch(reqs, tiling=tiling)
@@ -162,3 +162,13 @@ def test_graphs_off_matches(singles, monkeypatch):
     res, _ = _batch(reqs[:2])
     for r, q, ref in zip(res, reqs[:2], refs[:2]):
         _same(r, ref, q)
+
+
+def test_concurrent_streams_equal_single_solves(singles):
+    """The same solves as concurrent single-solve loops, one stream each,
+    some joining while others run."""
+    reqs, refs = singles
+    res, st = _batch(reqs, mode="streams", stagger=1)
+    for r, q, ref in zip(res, reqs, refs):
+        _same(r, ref, q)
+    assert st["launches"] >= 2 * sum(1 for q in reqs if q.adr is not None)

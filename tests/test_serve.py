@@ -44,13 +44,14 @@ def test_poisson_arrivals_are_seeded_and_increasing():
 
 
 @pytest.mark.gpu
-def test_served_results_equal_single_solves():
+@pytest.mark.parametrize("mode", ["streams", "tiles"])
+def test_served_results_equal_single_solves(mode):
     from prtlb_gpu import solve_adr, stokes_d3q19
     from prtlb_gpu.serve import poisson_arrivals, serve
     from prtlb_gpu.workloads import request_set
     reqs, draws = request_set(6, 14, 26, seed=5, nit=400, max_steps=1500, n_t=3)
     arrivals = poisson_arrivals(len(reqs), 40.0, seed=5)
-    srv = serve(reqs, arrivals, graph_steps=9)
+    srv = serve(reqs, arrivals, graph_steps=9, mode=mode)
     assert srv.summary["completed"] == len(reqs)
     assert srv.summary["latency_p99_s"] >= srv.summary["latency_p50_s"] > 0
     by = {r.tag: r for r in srv.results}
