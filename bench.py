@@ -377,7 +377,7 @@ def run_served(args, torch):
         solve_batch(small, quiet=True)
     torch.cuda.synchronize()
     with Clocks(0) as clk:
-        srv = serve(reqs, arrivals, mode=args.serve_mode)
+        srv = serve(reqs, arrivals, mode=args.serve_mode, flow_cap=args.flow_cap)
         torch.cuda.synchronize()
         # plain: one server, first come first served, same arrival times
         t0 = time.perf_counter()
@@ -399,8 +399,9 @@ def run_served(args, torch):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "served: %d requests, Poisson %.3g req/s, edge U{32..160}, "
-                                   "draws as the batched set, 80%% HBM admission, %s" % (
-                                       n, args.rate, args.serve_mode),
+                                   "draws as the batched set, 80%% HBM admission, flow phase "
+                                   "capped at %d pore voxels, %s" % (
+                                       n, args.rate, args.flow_cap, args.serve_mode),
                        "seed": SEED, "geometry_s": round(gen_s, 2)},
             "latency_p50_s": S["latency_p50_s"], "latency_p99_s": S["latency_p99_s"],
             "queue_p50_s": S["queue_p50_s"], "completed": S["completed"], "failed": S["failed"],
@@ -468,7 +469,8 @@ def main():
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"])
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--rate", type=float, default=20.0)
-    ap.add_argument("--serve-mode", default="streams", choices=["streams", "tiles"])
+    ap.add_argument("--serve-mode", default="tiles", choices=["streams", "tiles"])
+    ap.add_argument("--flow-cap", type=int, default=2000000)
     args = ap.parse_args()
     if args.mode != "plain" and args.impl == "ours":
         import torch

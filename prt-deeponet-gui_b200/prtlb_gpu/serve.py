@@ -94,14 +94,29 @@ class Served(object):
         }
 
 
+def pore_voxels(req):
+    """Pore voxels of a request (the flow solve's work per iteration)."""
+    n = getattr(req, "_pores", None)
+    if n is None:
+        n = req._pores = int(np.count_nonzero(req.mat == 2))
+    return n
+
+
 def serve(requests, arrivals, device=0, hbm_fraction=0.8, graph_steps=20, quiet=True,
-          budget_bytes=None, mode="streams"):
+          budget_bytes=None, mode="tiles", flow_cap=2000000):
     """Serve `requests` arriving at host times `arrivals` (seconds after the
     start).  Admission is first-come first-served while the summed
     footprints stay within hbm_fraction of the device memory (or
-    `budget_bytes`).  mode "streams" runs the admitted solves as concurrent
-    single-solve loops (StreamBatch), "tiles" through the batch engine's
-    tile-list kernels (Batch).  Returns a Served."""
+    `budget_bytes`) and the pore voxels of the solves in their flow phase
+    stay within `flow_cap` (enough flow work to keep the GPU's memory system
+    busy; a solve's transport phase is light and does not count, so new
+    flows start as soon as older ones reach their transport).  An arrival
+    that alone exceeds the cap is admitted when no flow is running.  Under
+    overload this keeps the GPU full while finishing requests nearly in
+    arrival order, instead of sharing the GPU among every queued request.
+    mode "tiles" advances the admitted solves with the batch engine's
+    tile-list kernels (Batch), "streams" as concurrent single-solve loops
+    (StreamBatch).  Returns a Served."""
     order = np.argsort(np.asarray(arrivals, np.float64), kind="stable")
     pending = collections.deque((float(arrivals[i]), requests[i]) for i in order)
     if budget_bytes is None:
@@ -127,11 +142,15 @@ def serve(requests, arrivals, device=0, hbm_fraction=0.8, graph_steps=20, quiet=
             # host work overlapping the launch: finished phases, admissions
             for res in b.process():
                 used -= reserved.pop(id(res), 0)
+            flow_load = sum(pore_voxels(j.req) for j in b._jobs.values() if j.phase == "flow")
             while waiting:
                 t_arr, req = waiting[0]
                 need = footprint(req)
                 if used + need > budget_bytes and used > 0:
                     break
+                if flow_cap and flow_load + pore_voxels(req) > flow_cap and flow_load > 0:
+                    break
+                flow_load += pore_voxels(req)
                 waiting.popleft()
                 try:
                     res = b.submit(req)

@@ -80,3 +80,17 @@ def test_admission_budget_serialises_when_tight():
     adm = sorted(r.t_admit for r in srv.results)
     done = sorted(r.t_done for r in srv.results)
     assert adm[1] >= done[0] - 1e-6 and adm[2] >= done[1] - 1e-6
+
+
+@pytest.mark.gpu
+def test_flow_cap_admits_the_next_flow_after_the_previous_one():
+    """With a flow cap of one voxel, a request is admitted only once the
+    previous request's flow phase has finished (its transport may still run)."""
+    from prtlb_gpu.serve import poisson_arrivals, serve
+    from prtlb_gpu.workloads import request_set
+    reqs, _ = request_set(3, 14, 18, seed=11, nit=300, max_steps=400, n_t=2)
+    srv = serve(reqs, poisson_arrivals(3, 200.0, seed=2), graph_steps=7, flow_cap=1)
+    assert srv.summary["completed"] == 3
+    rs = sorted(srv.results, key=lambda r: r.t_admit)
+    assert rs[1].t_admit >= rs[0].t_flow - 1e-6
+    assert rs[2].t_admit >= rs[1].t_flow - 1e-6
