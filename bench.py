@@ -412,6 +412,73 @@ def run_served(args, torch):
             "identical_to_plain": same, "clocks": clk.summary()}
 
 
+def _err(a, b, mask=None):
+    """(relative L2, max abs error / max |reference|) of a against b."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if mask is not None:
+        a, b = a[..., mask], b[..., mask]
+    nb = float(np.sqrt((b ** 2).sum()))
+    mb = float(np.abs(b).max())
+    return (float(np.sqrt(((a - b) ** 2).sum())) / nb if nb else 0.0,
+            float(np.abs(a - b).max()) / mb if mb else 0.0)
+
+
+def run_precision(args, torch):
+    """The precision sweep: flow stored in fp32 / fp32f / fp16 against the
+    fp64 solve (the reference's arithmetic) on sphere packs at 128^3 and
+    192^3 -- velocity, permeability -- and the float32 transport (reversible
+    sorption, K_d 0.5) driven by each field at Pe 1 / 10 / 100 against the
+    transport driven by the fp64 field.  (The float32 transport against its
+    float64 twin is a test: tests/test_sorption.py.)"""
+    from prtlb_gpu import _lib, solve_adr, stokes_d3q19
+    from prtlb_gpu.chemistry import reversible_sorption_chemistry
+    from prtlb_gpu.geometry import sphere_pack_3d
+    ctx = _lib.Context(0)
+    rows = []
+    q = contextlib.redirect_stdout(io.StringIO())
+    cases = [(128, 0.35), (128, 0.45), (128, 0.55), (192, 0.45)]
+    with Clocks(0) as clk, q:
+        for edge, phi in cases:
+            g = sphere_pack_3d(edge, phi, SEED)
+            m = g == 2
+            v, info = {}, {}
+            for prec in ("fp64", "fp32", "fp32f", "fp16"):
+                info[prec] = {}
+                v[prec] = stokes_d3q19(g, nit=FLOW_NIT, force=FORCE, tau_lb=TAU, tol=FLOW_TOL,
+                                       precision=prec, info=info[prec], ctx=ctx)
+            for prec in ("fp32", "fp32f", "fp16"):
+                l2, mx = _err(v[prec], v["fp64"], m)
+                k, k64 = info[prec]["permeability"], info["fp64"]["permeability"]
+                row = {"edge": edge, "porosity": phi, "precision": prec, "field": "velocity",
+                       "rel_l2": l2, "max_err": mx, "permeability_rel_err": abs(k - k64) / abs(k64),
+                       "flow_iters": info[prec]["flow_iters"],
+                       "flow_iters_fp64": info["fp64"]["flow_iters"]}
+                rows.append(row)
+            if edge == 128 and phi == 0.45:
+                chem = reversible_sorption_chemistry(0.5, 1.0)
+                for pe in (1.0, 10.0, 100.0):
+                    c = {}
+                    for prec in ("fp64", "fp32", "fp16"):
+                        c[prec], _ = solve_adr(g, v[prec], pe=pe, da=1.0, n_t=3, n_species=2,
+                                               chem=chem, steps=args.adr_sweep_steps, ctx=ctx)
+                    for prec in ("fp32", "fp16"):
+                        l2, mx = _err(c[prec][-1], c["fp64"][-1])
+                        rows.append({"edge": edge, "porosity": phi, "precision": prec,
+                                     "field": "concentration (sorption, Pe %g, %d steps)" % (
+                                         pe, args.adr_sweep_steps), "rel_l2": l2, "max_err": mx})
+    ctx.close()
+    worst = max(r["rel_l2"] for r in rows if r["precision"] == "fp32" and r["field"] == "velocity")
+    return {"metric": "fp32 velocity rel L2 vs fp64 (worst case)", "value": worst,
+            "unit": "relative L2", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "precision sweep: sphere packs 128^3 (porosity 0.35/0.45/0.55) "
+                                   "and 192^3 (0.45), r U[4,7], seed 0; flow to tol 1e-6 "
+                                   "(cap 30000)", "seed": SEED},
+            "rows": rows, "clocks": clk.summary()}
+
+
 # ---------------------------------------------------------------------------
 # CPU: the oracle (a restatement of the reference's NumPy algorithm)
 # ---------------------------------------------------------------------------
@@ -466,7 +533,9 @@ def main():
     ap.add_argument("--adr-steps", type=int, default=None)
     # solves-per-hour modes (each prints its own line; the default is the
     # plain 3D bench line)
-    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"])
+    ap.add_argument("--mode", default="plain",
+                    choices=["plain", "batched", "served", "precision"])
+    ap.add_argument("--adr-sweep-steps", type=int, default=3000)
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--serve-mode", default="tiles", choices=["streams", "tiles"])
@@ -474,7 +543,7 @@ def main():
     args = ap.parse_args()
     if args.mode != "plain" and args.impl == "ours":
         import torch
-        fn = run_batched if args.mode == "batched" else run_served
+        fn = {"batched": run_batched, "served": run_served, "precision": run_precision}[args.mode]
         print(json.dumps(fn(args, torch)))
         return
     globals().update(EDGE=args.edge, FLOW_NIT=args.flow_nit, ADR_STEPS=args.adr_steps)

@@ -137,3 +137,21 @@ def test_gpu_sorption_in_a_porous_flow_matches_oracle():
     assert info["dt"] == rinfo["dt"]
     assert np.array_equal(tn, rtn)
     assert np.array_equal(out, ref), float(np.abs(out - ref).max())
+
+
+@pytest.mark.gpu
+def test_gpu_float32_transport_against_float64_twin():
+    """The transport is float32 like the reference; its distance from the
+    same algorithm in float64 (the oracle's twin) on a 3D pack with flow and
+    sorption stays at float32 rounding level."""
+    from prtlb_gpu import solve_adr, sphere_pack_3d, stokes_d3q19
+    from prtlb_gpu.chemistry import reversible_sorption_chemistry
+    g = sphere_pack_3d(24, 0.45, 0)
+    with contextlib.redirect_stdout(io.StringIO()):
+        v = stokes_d3q19(g, nit=2000, tol=0.0, precision="fp64")
+    chem = reversible_sorption_chemistry(KD, 1.0)
+    c32, _, _ = _run(solve_adr, g, v, chem, 600, 10.0)
+    c64, _, _ = _run(_oracle(np.float64), g, v, chem, 600, 10.0)
+    d = c32.astype(np.float64) - c64
+    rel = float(np.sqrt((d ** 2).sum() / (c64 ** 2).sum()))
+    assert rel < 1e-5, rel
