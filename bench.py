@@ -62,9 +62,10 @@ POROSITY = 0.45
 SEED = 0
 FORCE, TAU, FLOW_TOL, FLOW_NIT = 2e-6, 0.8, 1e-6, 30000
 ADR_STEPS = None  # None: run to the reference's stop rule
-# DRAM bytes (read + write) of one lb_step_kernel launch from an ncu capture,
-# by grid edge (profiles/lb_step_kernel_plain3d.md); None until captured
-TRAFFIC_PER_LAUNCH = {64: 35480000}
+# DRAM bytes (read + write) of one lb_step_kernel launch from an ncu capture
+# (cache flushed before the launch), by grid edge: profiles/
+# lb_step_kernel_plain3d_64.md and lb_step_kernel_sphere128.md
+TRAFFIC_PER_LAUNCH = {64: 18231808, 128: 177509632}
 PE, DA, KS, N_T = 10.0, 1.0, 0.5, 5
 METRIC = "D3Q19 TRT+ADR GLUPS"
 UNIT = "GLUPS"
