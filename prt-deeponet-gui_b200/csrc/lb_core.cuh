@@ -155,12 +155,10 @@ __device__ __forceinline__ void upstream_slots(const FlowMap& fm, const Grid& g,
 // comment).  Lattices hold the pore voxels only, in C order: voxel
 // cells[k] is slot k, and imap[voxel] is the slot of a pore voxel or -1.
 template <class L, class S>
-__device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __restrict__ lw, int k,
-                                       const FlowMap& fm, const Grid& g, float inv,
-                                       typename Pop<S>::H (&h)[L::Q]) {
-    const long long NF = fm.nf;
-    int src[L::Q];
-    upstream_slots<L>(fm, g, k, src);
+__device__ __forceinline__ void gather_from_slots(const S* __restrict__ lr,
+                                                  const S* __restrict__ lw, int k, long long NF,
+                                                  const int (&src)[L::Q], float inv,
+                                                  typename Pop<S>::H (&h)[L::Q]) {
     h[0] = Pop<S>::ld(lr + k, inv);
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
@@ -168,6 +166,24 @@ __device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __rest
                            : Pop<S>::ld(lw + (long long)L::opp(i) * NF + k, inv);
     }
 }
+
+template <class L, class S>
+__device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __restrict__ lw, int k,
+                                       const FlowMap& fm, const Grid& g, float inv,
+                                       typename Pop<S>::H (&h)[L::Q]) {
+    int src[L::Q];
+    upstream_slots<L>(fm, g, k, src);
+    gather_from_slots<L, S>(lr, lw, k, fm.nf, src, inv, h);
+}
+
+// Programmatic dependent launch: let the next kernel in the stream start
+// launching now, and wait until the previous one has finished and its
+// stores are visible (both no-ops for a kernel launched without the
+// programmatic-serialisation attribute).
+__device__ __forceinline__ void griddep_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" :::);
+}
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 constexpr int kFlowThreads = 256;
 
@@ -199,10 +215,8 @@ struct Staged {
 // but no register is held while a load is in flight.
 template <class L, class S>
 __device__ __forceinline__ void gather_staged(const S* __restrict__ lr, const S* __restrict__ lw,
-                                              int k, const FlowMap& fm, const Grid& g, S* col) {
-    const long long NF = fm.nf;
-    int src[L::Q];
-    upstream_slots<L>(fm, g, k, src);
+                                              int k, long long NF, const int (&src)[L::Q],
+                                              S* col) {
     cp_async_pop(col, lr + k);
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
@@ -287,30 +301,41 @@ __device__ __forceinline__ void collide_store(S* __restrict__ lw, int c, long lo
 }
 
 // One pore voxel (slot k) of one LB iteration from read lattice lr into
-// write lattice lw: gather, moments, collision, store; returns |u_x| for
-// the convergence mean.
+// write lattice lw, its upstream slots already found: gather, moments,
+// collision, store; returns |u_x| for the convergence mean.
 template <class L, class M>
-__device__ __forceinline__ double lb_cell_rw(const typename M::S* __restrict__ lr,
-                                             typename M::S* __restrict__ lw, const FlowMap& fm,
-                                             const Grid& g, const LbParams& kc, int k) {
+__device__ __forceinline__ double lb_cell_slots(const typename M::S* __restrict__ lr,
+                                                typename M::S* __restrict__ lw, const FlowMap& fm,
+                                                const LbParams& kc, int k,
+                                                const int (&src)[L::Q]) {
     using S = typename M::S;
     using R = typename M::R;
     using RA = typename M::RA;
     if constexpr (M::staged) {
         __shared__ S stage[L::Q * kFlowThreads];
         S* col = stage + threadIdx.x;
-        gather_staged<L, S>(lr, lw, k, fm, g, col);
+        gather_staged<L, S>(lr, lw, k, fm.nf, src, col);
         const Staged<S> h{col};
         const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
         collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
         return fabs((double)m.jx * (double)m.inv_rho);
     } else {
         typename Pop<S>::H h[L::Q];
-        gather<L, S>(lr, lw, k, fm, g, kc.inv_scale, h);
+        gather_from_slots<L, S>(lr, lw, k, fm.nf, src, kc.inv_scale, h);
         const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
         collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
         return fabs((double)m.jx * (double)m.inv_rho);
     }
+}
+
+// The same, finding the upstream slots first.
+template <class L, class M>
+__device__ __forceinline__ double lb_cell_rw(const typename M::S* __restrict__ lr,
+                                             typename M::S* __restrict__ lw, const FlowMap& fm,
+                                             const Grid& g, const LbParams& kc, int k) {
+    int src[L::Q];
+    upstream_slots<L>(fm, g, k, src);
+    return lb_cell_slots<L, M>(lr, lw, fm, kc, k, src);
 }
 
 // The same with the lattice pair chosen by the iteration parity: iteration

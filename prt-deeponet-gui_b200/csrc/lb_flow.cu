@@ -21,6 +21,8 @@
 // Populations are stored shifted, h_i = f_i - w_i: the non-equilibrium part
 // that carries the viscous stress is of the order of the force (1e-7) and
 // would drown next to w_i ~ 0.3 in float32 (prtlb_2d.py:354-362).
+#include <cstdlib>
+
 #include "lb_core.cuh"
 
 namespace prt {
@@ -31,12 +33,19 @@ template <class L, class M, bool ODD, bool CHECK>
 __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
     lb_step_kernel(typename M::S* __restrict__ f, FlowMap fm, Grid g, LbParams kc,
                    const FlowCtrl* __restrict__ ctrl, int kstep, double* __restrict__ partials) {
+    griddep_launch_dependents();
+    const int k = blockIdx.x * kFlowThreads + threadIdx.x;
+    // the pore maps never change during a solve: the upstream slots are
+    // looked up while the previous iteration may still be running
+    int src[L::Q];
+    if (k < fm.nf) upstream_slots<L>(fm, g, k, src);
+    griddep_wait();
     const long long it = ctrl->it_base + kstep;
     if (ctrl->done || it >= ctrl->nit) return;  // uniform over the grid
-    const int k = blockIdx.x * kFlowThreads + threadIdx.x;
     double acc = 0.0;
     if (k < fm.nf) {
-        const double ux = lb_cell<L, M, ODD>(f, fm, g, kc, k);
+        const long long QN = (long long)L::Q * fm.nf;
+        const double ux = lb_cell_slots<L, M>(ODD ? f + QN : f, ODD ? f : f + QN, fm, kc, k, src);
         if (CHECK) acc = ux;
     }
     if (CHECK) block_sum_store(acc, partials + blockIdx.x);
@@ -195,18 +204,45 @@ __global__ void imap_scatter_kernel(int* __restrict__ cells, int nf, int* __rest
 // -------------------------------------------------------------------------
 int flow_blocks(long long n) { return (int)((n + kFlowThreads - 1) / kFlowThreads); }
 
+// Step kernels go out with programmatic stream serialisation: kernel t+1
+// starts while kernel t drains and waits in griddepcontrol.wait for its
+// results (PRT_PDL=0 launches them plainly).
+static bool pdl_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("PRT_PDL");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
+template <class L, class M, bool ODD, bool CHECK>
+static cudaError_t launch_step_one(typename M::S* f, const FlowMap& fm, const Grid& g,
+                                   const LbParams& k, const FlowCtrl* ctrl, int kstep,
+                                   double* partials, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(flow_blocks(fm.nf));
+    cfg.blockDim = dim3(kFlowThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, lb_step_kernel<L, M, ODD, CHECK>, f, fm, g, k, ctrl, kstep,
+                              partials);
+}
+
 template <class L, class M>
 static cudaError_t launch_step_t(bool odd, bool check, void* f, const FlowMap& fm,
                                  const Grid& g, const LbParams& k, const FlowCtrl* ctrl, int kstep,
                                  double* partials, cudaStream_t s) {
     if (fm.nf <= 0) return cudaSuccess;
-    dim3 grid(flow_blocks(fm.nf));
     typename M::S* fs = static_cast<typename M::S*>(f);
-    if (!odd && !check) lb_step_kernel<L, M, false, false><<<grid, kFlowThreads, 0, s>>>(fs, fm, g, k, ctrl, kstep, partials);
-    if (!odd && check) lb_step_kernel<L, M, false, true><<<grid, kFlowThreads, 0, s>>>(fs, fm, g, k, ctrl, kstep, partials);
-    if (odd && !check) lb_step_kernel<L, M, true, false><<<grid, kFlowThreads, 0, s>>>(fs, fm, g, k, ctrl, kstep, partials);
-    if (odd && check) lb_step_kernel<L, M, true, true><<<grid, kFlowThreads, 0, s>>>(fs, fm, g, k, ctrl, kstep, partials);
-    return cudaGetLastError();
+    if (!odd && !check) return launch_step_one<L, M, false, false>(fs, fm, g, k, ctrl, kstep, partials, s);
+    if (!odd && check) return launch_step_one<L, M, false, true>(fs, fm, g, k, ctrl, kstep, partials, s);
+    if (odd && !check) return launch_step_one<L, M, true, false>(fs, fm, g, k, ctrl, kstep, partials, s);
+    return launch_step_one<L, M, true, true>(fs, fm, g, k, ctrl, kstep, partials, s);
 }
 
 #define PRT_DISPATCH(FN, ...)                                                        \
