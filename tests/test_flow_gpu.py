@@ -132,3 +132,15 @@ def test_permeability_of_a_slit():
     stokes_d2q9(g, nit=60000, force=2e-6, tau_lb=0.8, tol=1e-9, info=info)
     k_exact = (H * H + 0.5) * H / (12.0 * (H + 2))
     assert abs(info["permeability"] / k_exact - 1) < 0.01, (info["permeability"], k_exact)
+
+
+def test_programmatic_dependent_launch_gives_the_same_field(monkeypatch):
+    """The optional programmatic-dependent-launch mode of the step kernels
+    (PRT_PDL=1) changes when a kernel starts, never what it computes."""
+    from prtlb_gpu import sphere_pack_3d, stokes_d3q19
+    g = sphere_pack_3d(24, 0.45, 0)
+    with contextlib.redirect_stdout(io.StringIO()):
+        ref = stokes_d3q19(g, nit=400, tol=0.0, precision="fp32")
+        monkeypatch.setenv("PRT_PDL", "1")
+        got = stokes_d3q19(g, nit=400, tol=0.0, precision="fp32")
+    assert np.array_equal(got, ref)
