@@ -44,15 +44,12 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
             continue;
         }
         const int nf = sj.fm.nf;
-        const long long QN = (long long)L::Q * nf;
-        S* f = static_cast<S*>(sj.f);
-        const S* lr = (it & 1) ? f + QN : f;
-        S* lw = (it & 1) ? f : f + QN;
+        const Lat<S> lat = lattices<L>(static_cast<S*>(sj.f), nf, (it & 1) != 0);
 #pragma unroll 1
         for (int b = tl.b0; b < tl.b0 + tl.nb; ++b) {
             const int k = b * kFlowThreads + threadIdx.x;
             double acc = 0.0;
-            if (k < nf) acc = lb_cell_rw<L, M>(lr, lw, sj.fm, sj.g, sj.kc, k);
+            if (k < nf) acc = lb_cell_rw<L, M>(lat, sj.fm, sj.g, sj.kc, k);
             if (check) block_sum_store(acc, sj.partials + b);
         }
         // every warp has read the control block and finished its voxels

@@ -154,26 +154,42 @@ __device__ __forceinline__ void upstream_slots(const FlowMap& fm, const Grid& g,
 // Gather the arrived populations of pore voxel number k (see the file
 // comment).  Lattices hold the pore voxels only, in C order: voxel
 // cells[k] is slot k, and imap[voxel] is the slot of a pore voxel or -1.
+// The two lattices of a solve as one array and 32-bit element offsets: the
+// read lattice starts at element rd, the write lattice at wr (0 or Q*nf
+// each; 2*Q*nf < 2^31 is checked at set-up), so every address is one
+// 32-bit index and one wide multiply-add off the base.
+template <class S>
+struct Lat {
+    S* f;
+    int rd, wr, nf;
+    __device__ const S* in(int i, int slot) const { return f + (rd + i * nf + slot); }
+    __device__ S* out(int i, int slot) const { return f + (wr + i * nf + slot); }
+};
+
 template <class L, class S>
-__device__ __forceinline__ void gather_from_slots(const S* __restrict__ lr,
-                                                  const S* __restrict__ lw, int k, long long NF,
+__device__ __forceinline__ Lat<S> lattices(S* f, int nf, bool odd) {
+    const int qn = L::Q * nf;
+    return Lat<S>{f, odd ? qn : 0, odd ? 0 : qn, nf};
+}
+
+template <class L, class S>
+__device__ __forceinline__ void gather_from_slots(const Lat<S>& lat, int k,
                                                   const int (&src)[L::Q], float inv,
                                                   typename Pop<S>::H (&h)[L::Q]) {
-    h[0] = Pop<S>::ld(lr + k, inv);
+    h[0] = Pop<S>::ld(lat.in(0, k), inv);
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
-        h[i] = src[i] >= 0 ? Pop<S>::ld(lr + (long long)i * NF + src[i], inv)
-                           : Pop<S>::ld(lw + (long long)L::opp(i) * NF + k, inv);
+        // a rock upstream neighbour: x's own value of two iterations back
+        h[i] = Pop<S>::ld(src[i] >= 0 ? lat.in(i, src[i]) : lat.out(L::opp(i), k), inv);
     }
 }
 
 template <class L, class S>
-__device__ __forceinline__ void gather(const S* __restrict__ lr, const S* __restrict__ lw, int k,
-                                       const FlowMap& fm, const Grid& g, float inv,
-                                       typename Pop<S>::H (&h)[L::Q]) {
+__device__ __forceinline__ void gather(const Lat<S>& lat, int k, const FlowMap& fm, const Grid& g,
+                                       float inv, typename Pop<S>::H (&h)[L::Q]) {
     int src[L::Q];
     upstream_slots<L>(fm, g, k, src);
-    gather_from_slots<L, S>(lr, lw, k, fm.nf, src, inv, h);
+    gather_from_slots<L, S>(lat, k, src, inv, h);
 }
 
 // Programmatic dependent launch: let the next kernel in the stream start
@@ -214,15 +230,14 @@ struct Staged {
 // thread's column of a [Q][kFlowThreads] shared array): the same sources,
 // but no register is held while a load is in flight.
 template <class L, class S>
-__device__ __forceinline__ void gather_staged(const S* __restrict__ lr, const S* __restrict__ lw,
-                                              int k, long long NF, const int (&src)[L::Q],
+__device__ __forceinline__ void gather_staged(const Lat<S>& lat, int k, const int (&src)[L::Q],
                                               S* col) {
-    cp_async_pop(col, lr + k);
+    cp_async_pop(col, lat.in(0, k));
 #pragma unroll
     for (int i = 1; i < L::Q; ++i) {
-        const S* p = src[i] >= 0 ? lr + (long long)i * NF + src[i]
-                                 : lw + (long long)L::opp(i) * NF + k;
-        cp_async_pop(col + i * kFlowThreads, p);
+        const int off = src[i] >= 0 ? lat.rd + i * lat.nf + src[i]
+                                    : lat.wr + L::opp(i) * lat.nf + k;
+        cp_async_pop(col + i * kFlowThreads, lat.f + off);
     }
     cp_async_wait_all();
 }
@@ -270,14 +285,13 @@ __device__ __forceinline__ Moments<R, RA> moments(const HA& h, double half_g) {
 // the symmetric one.  The new population is h + delta with delta summed
 // first, so the stored result rounds once; it goes to slot i of voxel c.
 template <class L, class S, class R, class RA, class HA>
-__device__ __forceinline__ void collide_store(S* __restrict__ lw, int c, long long N,
-                                              const HA& h, const Moments<R, RA>& m,
-                                              const LbParams& kc) {
+__device__ __forceinline__ void collide_store(const Lat<S>& lat, int c, const HA& h,
+                                              const Moments<R, RA>& m, const LbParams& kc) {
     const R omp = R(kc.omp);
     const R inv_rho = R(m.inv_rho);
     const R heq0 = R(L::w(0)) * (m.drho - R(1.5) * m.jsq);
     const R h0 = R(h[0]);
-    Pop<S>::st(lw + c, h0 - omp * (h0 - heq0), kc.scale);
+    Pop<S>::st(lat.out(0, c), h0 - omp * (h0 - heq0), kc.scale);
 #pragma unroll
     for (int p = 0; p < L::NP; ++p) {
         const int a = L::pa(p), b = L::pb(p);
@@ -295,56 +309,44 @@ __device__ __forceinline__ void collide_store(S* __restrict__ lw, int c, long lo
         const RA dma = RA(kc.omm) * (RA(0.5) * (RA(h[a]) - RA(h[b])) - RA(3.0 * L::w(a)) * eJ);
         const R dm = R(dma);
         const R gp = R(kc.guo[p]);
-        Pop<S>::st(lw + (long long)a * N + c, ha + ((gp - dp) - dm), kc.scale);
-        Pop<S>::st(lw + (long long)b * N + c, hb + ((dm - dp) - gp), kc.scale);
+        Pop<S>::st(lat.out(a, c), ha + ((gp - dp) - dm), kc.scale);
+        Pop<S>::st(lat.out(b, c), hb + ((dm - dp) - gp), kc.scale);
     }
 }
 
-// One pore voxel (slot k) of one LB iteration from read lattice lr into
-// write lattice lw, its upstream slots already found: gather, moments,
+// One pore voxel (slot k) of one LB iteration from the read lattice into
+// the write lattice, its upstream slots already found: gather, moments,
 // collision, store; returns |u_x| for the convergence mean.
 template <class L, class M>
-__device__ __forceinline__ double lb_cell_slots(const typename M::S* __restrict__ lr,
-                                                typename M::S* __restrict__ lw, const FlowMap& fm,
-                                                const LbParams& kc, int k,
-                                                const int (&src)[L::Q]) {
+__device__ __forceinline__ double lb_cell_slots(const Lat<typename M::S>& lat, const LbParams& kc,
+                                                int k, const int (&src)[L::Q]) {
     using S = typename M::S;
     using R = typename M::R;
     using RA = typename M::RA;
     if constexpr (M::staged) {
         __shared__ S stage[L::Q * kFlowThreads];
         S* col = stage + threadIdx.x;
-        gather_staged<L, S>(lr, lw, k, fm.nf, src, col);
+        gather_staged<L, S>(lat, k, src, col);
         const Staged<S> h{col};
         const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
-        collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
+        collide_store<L, S, R, RA>(lat, k, h, m, kc);
         return fabs((double)m.jx * (double)m.inv_rho);
     } else {
         typename Pop<S>::H h[L::Q];
-        gather_from_slots<L, S>(lr, lw, k, fm.nf, src, kc.inv_scale, h);
+        gather_from_slots<L, S>(lat, k, src, kc.inv_scale, h);
         const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
-        collide_store<L, S, R, RA>(lw, k, fm.nf, h, m, kc);
+        collide_store<L, S, R, RA>(lat, k, h, m, kc);
         return fabs((double)m.jx * (double)m.inv_rho);
     }
 }
 
 // The same, finding the upstream slots first.
 template <class L, class M>
-__device__ __forceinline__ double lb_cell_rw(const typename M::S* __restrict__ lr,
-                                             typename M::S* __restrict__ lw, const FlowMap& fm,
+__device__ __forceinline__ double lb_cell_rw(const Lat<typename M::S>& lat, const FlowMap& fm,
                                              const Grid& g, const LbParams& kc, int k) {
     int src[L::Q];
     upstream_slots<L>(fm, g, k, src);
-    return lb_cell_slots<L, M>(lr, lw, fm, kc, k, src);
-}
-
-// The same with the lattice pair chosen by the iteration parity: iteration
-// t reads lattice (t & 1) and writes the other one.
-template <class L, class M, bool ODD>
-__device__ __forceinline__ double lb_cell(typename M::S* __restrict__ f, const FlowMap& fm,
-                                          const Grid& g, const LbParams& kc, int k) {
-    const long long QN = (long long)L::Q * fm.nf;
-    return lb_cell_rw<L, M>(ODD ? f + QN : f, ODD ? f : f + QN, fm, g, kc, k);
+    return lb_cell_slots<L, M>(lat, kc, k, src);
 }
 
 // Block sum of one double per thread (warp shuffles, then the warp sums in

@@ -44,8 +44,7 @@ __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
     if (ctrl->done || it >= ctrl->nit) return;  // uniform over the grid
     double acc = 0.0;
     if (k < fm.nf) {
-        const long long QN = (long long)L::Q * fm.nf;
-        const double ux = lb_cell_slots<L, M>(ODD ? f + QN : f, ODD ? f : f + QN, fm, kc, k, src);
+        const double ux = lb_cell_slots<L, M>(lattices<L>(f, fm.nf, ODD), kc, k, src);
         if (CHECK) acc = ux;
     }
     if (CHECK) block_sum_store(acc, partials + blockIdx.x);
@@ -84,9 +83,7 @@ __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
     using R = typename M::R;
     using RA = typename M::RA;
     const int kk = blockIdx.x * kFlowThreads + threadIdx.x;
-    const long long QN = (long long)L::Q * fm.nf;
-    const S* lr = ODD ? f + QN : f;
-    const S* lw = ODD ? f : f + QN;
+    const Lat<S> lat = lattices<L>(const_cast<S*>(f), fm.nf, ODD);
     double sux = 0.0, srho = 0.0, ssp = 0.0, mx = 0.0, nonf = 0.0;
     if (kk < fm.nf) {
         // solid voxels of vel were zeroed before this launch
@@ -96,7 +93,7 @@ __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
         float vx = 0.f, vy = 0.f, vz = 0.f;
         {
             typename Pop<S>::H h[L::Q];
-            gather<L, S>(lr, lw, kk, fm, g, k.inv_scale, h);
+            gather<L, S>(lat, kk, fm, g, k.inv_scale, h);
             const Moments<R, RA> m = moments<L, R, RA>(h, k.half_g);
             const RA ux = m.jx * m.inv_rho, uy = m.jy * m.inv_rho, uz = m.jz * m.inv_rho;
             vx = (float)ux;

@@ -195,6 +195,8 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
     NCK(cudaStreamSynchronize(s));
     NCK(adr_launch_compact(flag, g.n, cnt, count, cells, s));
     NCK(cudaMemsetAsync(imap, 0xff, (size_t)g.n * 4, s));
+    if ((long long)2 * Q * nfluid >= (1ll << 31))
+        return fail(PRT_E_INVALID, "more pore voxels than the 32-bit lattice offsets hold");
     FlowMap fm;
     fm.ys = coord_bits(g.nz);
     fm.xs = fm.ys + coord_bits(g.ny);

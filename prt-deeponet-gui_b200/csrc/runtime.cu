@@ -143,6 +143,9 @@ int prt::flow_setup(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p
     CK(flow_launch_imap(F.cells.as<int>(), (int)nfluid, F.fluid.as<int>(), g, F.fm.ys, F.fm.xs,
                         s));
     ctx->launches += 7;
+    if ((long long)2 * Q * nfluid >= (1ll << 31))
+        return fail(ctx, PRT_E_INVALID,
+                    "more pore voxels than the 32-bit lattice offsets hold (2 Q nf >= 2^31)");
     F.fm.nf = (int)nfluid;
     F.fm.cells = F.cells.as<int>();
     F.fm.imap = F.fluid.as<int>();
