@@ -39,14 +39,15 @@ struct Axes<2> {  // a 2D grid (nx, ny) is stored as (nx, 1, ny)
     __host__ __device__ static constexpr int ax(int i) { return i == 0 ? 0 : 2; }
 };
 
+// Index arithmetic is 32-bit: a transport grid holds fewer than 2^31
+// values per buffer (ns x voxels, checked when the run begins).
 struct VoxelPos {
     int p[3];
-    long long c;
+    int c;
 };
 
-// Coordinates of voxel c (grids hold fewer than 2^31 voxels, so 32-bit
-// division is exact).
-__device__ __forceinline__ VoxelPos voxel_pos(long long c, const Grid& g) {
+// Coordinates of voxel c.
+__device__ __forceinline__ VoxelPos voxel_pos(int c, const Grid& g) {
     VoxelPos v;
     v.c = c;
     unsigned t = (unsigned)c;
@@ -69,24 +70,24 @@ __device__ __forceinline__ float ld_early(const float* p) {
 __device__ __forceinline__ int extent(const Grid& g, int a) {
     return a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
 }
-__device__ __forceinline__ long long stride(const Grid& g, int a) {
-    return a == 0 ? (long long)g.ny * g.nz : (a == 1 ? (long long)g.nz : 1ll);
+__device__ __forceinline__ int stride(const Grid& g, int a) {
+    return a == 0 ? g.ny * g.nz : (a == 1 ? g.nz : 1);
 }
 // index of the low face of voxel v along axis a in the (n_a + 1)-long face array
-__device__ __forceinline__ long long face_lo(const Grid& g, const VoxelPos& v, int a) {
+__device__ __forceinline__ int face_lo(const Grid& g, const VoxelPos& v, int a) {
     if (a == 0) return v.c;
-    if (a == 1) return ((long long)v.p[0] * (g.ny + 1) + v.p[1]) * g.nz + v.p[2];
-    return ((long long)v.p[0] * g.ny + v.p[1]) * (g.nz + 1) + v.p[2];
+    if (a == 1) return (v.p[0] * (g.ny + 1) + v.p[1]) * g.nz + v.p[2];
+    return (v.p[0] * g.ny + v.p[1]) * (g.nz + 1) + v.p[2];
 }
-__device__ __forceinline__ long long face_step(const Grid& g, int a) {
-    return a == 0 ? (long long)g.ny * g.nz : (a == 1 ? (long long)g.nz : 1ll);
+__device__ __forceinline__ int face_step(const Grid& g, int a) {
+    return a == 0 ? g.ny * g.nz : (a == 1 ? g.nz : 1);
 }
 
 // A neighbour value of chemical j.  Every neighbour that is actually read is a
 // solute voxel (the open / far flags guarantee it), so it is on the inlet
 // plane exactly when its x is 0; there the pinned feed replaces the stored
 // value (step(), prtlb_3d.py:1392-1400, pins before transport).
-__device__ __forceinline__ float ld_c(const float* __restrict__ Cj, long long c, int x, bool pin,
+__device__ __forceinline__ float ld_c(const float* __restrict__ Cj, int c, int x, bool pin,
                                       float feed) {
     const float v = ld_early(Cj + c);
     return (pin && x == 0) ? feed : v;
@@ -105,7 +106,7 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
         const int a = Axes<ND>::ax(i);
         const int p = v.p[a];
         const int n = extent(g, a);
-        const long long s = stride(g, a);
+        const int s = stride(g, a);
         const bool oL = fl & f_open_lo(a), oH = fl & f_open_hi(a);
         const bool fL = fl & f_far_lo(a), fH = fl & f_far_hi(a);
         // clamped (edge-replicated) neighbour positions
@@ -116,11 +117,11 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
         const int xp1 = (a == 0) ? pp1 : x0, xp2 = (a == 0) ? pp2 : x0;
         // all four neighbours and both faces are loaded before the flags
         // choose among them (clamped addresses are always in the grid)
-        const float vm1 = ld_c(Cj, v.c + (long long)(pm1 - p) * s, xm1, pin, feed);
-        const float vp1 = ld_c(Cj, v.c + (long long)(pp1 - p) * s, xp1, pin, feed);
-        const float vm2 = ld_c(Cj, v.c + (long long)(pm2 - p) * s, xm2, pin, feed);
-        const float vp2 = ld_c(Cj, v.c + (long long)(pp2 - p) * s, xp2, pin, feed);
-        const long long fi = face_lo(g, v, a);
+        const float vm1 = ld_c(Cj, v.c + (pm1 - p) * s, xm1, pin, feed);
+        const float vp1 = ld_c(Cj, v.c + (pp1 - p) * s, xp1, pin, feed);
+        const float vm2 = ld_c(Cj, v.c + (pm2 - p) * s, xm2, pin, feed);
+        const float vp2 = ld_c(Cj, v.c + (pp2 - p) * s, xp2, pin, feed);
+        const int fi = face_lo(g, v, a);
         const float uL = ld_early(face[a] + fi);
         const float uH = ld_early(face[a] + fi + face_step(g, a));
         const float Cm1 = oL ? vm1 : Cc;
@@ -214,9 +215,9 @@ __device__ __forceinline__ void reaction(const float (&C)[NS], float surf,
 template <int ND, int NS>
 __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params& p, long long n,
                                           long long kk) {
-    const long long c = d.idx[kk];
+    const int c = d.idx[kk];
     const uint32_t fl = d.flags[c];
-    const long long N = d.g.n;
+    const int N = (int)d.g.n;
     const float* __restrict__ Cin = d.buf[(n - 1) & 1];
     float* __restrict__ Cout = d.buf[n & 1];
     const VoxelPos v = voxel_pos(c, d.g);
@@ -225,7 +226,7 @@ __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params&
 #pragma unroll
     for (int j = 0; j < NS; ++j) {
         const bool pin = (p.pinned_mask >> j) & 1u;
-        C[j] = (pin && x0) ? p.feed[j] : Cin[(long long)j * N + c];
+        C[j] = (pin && x0) ? p.feed[j] : Cin[j * N + c];
     }
     float T[NS];
 #pragma unroll
@@ -234,7 +235,7 @@ __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params&
         if ((p.moving_mask >> j) & 1u) {
             const bool pin = (p.pinned_mask >> j) & 1u;
             const float dj[3] = {p.dface[j][0], p.dface[j][1], p.dface[j][2]};
-            T[j] = transport_one<ND>(Cin + (long long)j * N, d.g, v, fl, d.face, C[j], pin,
+            T[j] = transport_one<ND>(Cin + j * N, d.g, v, fl, d.face, C[j], pin,
                                      p.feed[j], dj);
         }
     }
@@ -259,8 +260,8 @@ __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params&
         const float rhs = mv ? (T[j] + dC[j]) : dC[j];
         float cn = C[j] + p.dt * rhs;
         cn = np_max(cn, 0.f);
-        Cout[(long long)j * N + c] = cn;
-        if (lad) lad[(long long)j * N + c] = cn;
+        Cout[j * N + c] = cn;
+        if (lad) lad[j * N + c] = cn;
     }
 }
 

@@ -527,6 +527,9 @@ extern "C" int prt_adr_begin(prt_ctx* ctx, const prt_adr_params* p) {
     if (p->ns < 1 || p->ns > PRT_MAX_SPECIES)
         return fail(ctx, PRT_E_INVALID, "between 1 and 8 chemicals are supported");
     if (!(p->dt > 0.f)) return fail(ctx, PRT_E_INVALID, "the time step must be positive");
+    if ((long long)p->ns * (A.d.g.n + A.d.g.n / std::max(1, A.d.g.nx) + 1) >= (1ll << 31))
+        return fail(ctx, PRT_E_INVALID,
+                    "chemicals x voxels too large for the transport's 32-bit indices");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
     A.graph.release();
