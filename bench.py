@@ -65,7 +65,7 @@ ADR_STEPS = None  # None: run to the reference's stop rule
 # DRAM bytes (read + write) of one lb_step_kernel launch from an ncu capture
 # (cache flushed before the launch), by grid edge: profiles/
 # lb_step_kernel_plain3d_64.md and lb_step_kernel_sphere128.md
-TRAFFIC_PER_LAUNCH = {64: 18231808, 128: 177509632}
+TRAFFIC_PER_LAUNCH = {64: 18238464, 128: 178001408}
 PE, DA, KS, N_T = 10.0, 1.0, 0.5, 5
 METRIC = "D3Q19 TRT+ADR GLUPS"
 UNIT = "GLUPS"
@@ -252,7 +252,7 @@ def run_ours(args, rank, world, torch, dist):
     value = replicas_value(updates, world, total_ms)
 
     # e2e: the drop-in API on host arrays
-    e2e_ms = []
+    e2e_ms, e2e_split = [], []
     h2d = d2h = 0
     with contextlib.redirect_stdout(io.StringIO()):
         for k in range(max(1, min(args.steps, 3))):
@@ -261,17 +261,25 @@ def run_ours(args, rank, world, torch, dist):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
+            w0 = time.perf_counter()
             v = stokes_d3q19(g, nit=FLOW_NIT, force=FORCE, tau_lb=TAU, tol=FLOW_TOL,
                              precision="fp32", ctx=ctx)
+            w1 = time.perf_counter()
+            tf = ctx.timing()
             out, tn = solve_adr(g, v, pe=PE, da=DA, n_t=N_T, n_species=1, chem=chem, ctx=ctx,
                                 steps=ADR_STEPS)
+            w2 = time.perf_counter()
+            ta = ctx.timing()
             e1.record(stream)
             e1.synchronize()
             e2e_ms.append(e0.elapsed_time(e1))
+            # host seconds of each call next to its device loop
+            e2e_split.append({"flow_call_ms": (w1 - w0) * 1e3, "flow_loop_ms": tf[0],
+                              "adr_call_ms": (w2 - w1) * 1e3, "adr_loop_ms": ta[2]})
     h2d = g.nbytes + g.nbytes + v.nbytes           # flow: mat; transport: mat + vel
     d2h = v.nbytes + out.nbytes                    # flow: vel; transport: snapshots
     e2e_updates = float(iters[0] + nsteps[0]) * ncell
-    e2e_value = e2e_updates * world / (statistics.mean(e2e_ms) * 1e-3) / 1e9
+    e2e_value = e2e_updates * world / (statistics.median(e2e_ms) * 1e-3) / 1e9
 
     # roofline of the dominant kernel from this run's own events
     fl_ms = statistics.mean(flow_ms)
@@ -290,7 +298,7 @@ def run_ours(args, rank, world, torch, dist):
     res = {"ms_per_step": total_ms / args.steps, "value": value, "e2e": e2e_value,
            "h2d": h2d, "d2h": d2h, "launches": launches, "roof": roof, "clocks": clk.summary(),
            "flow_ms": fl_ms, "adr_ms": ad_ms, "iters": iters[0], "adr_steps": nsteps[0],
-           "ncell": ncell, "nfluid": nfluid}
+           "ncell": ncell, "nfluid": nfluid, "e2e_ms": e2e_ms, "e2e_split": e2e_split}
     ctx.close()
     return res
 
@@ -337,13 +345,13 @@ def run_batched(args, torch):
     torch.cuda.synchronize()
     with Clocks(0) as clk:
         t0 = time.perf_counter()
-        res = solve_batch(reqs, quiet=True, mode="streams")
+        res = solve_batch(reqs, quiet=True, mode="tiles")
         torch.cuda.synchronize()
         t_batch = time.perf_counter() - t0
         t0 = time.perf_counter()
-        res_tiles = solve_batch(reqs, quiet=True, mode="tiles")
+        res_streams = solve_batch(reqs, quiet=True, mode="streams")
         torch.cuda.synchronize()
-        t_tiles = time.perf_counter() - t0
+        t_streams = time.perf_counter() - t0
         t0 = time.perf_counter()
         ref = [plain_solve(r, ctx) for r in reqs]
         torch.cuda.synchronize()
@@ -361,11 +369,11 @@ def run_batched(args, torch):
                                    "order / reversible sorption, D3Q19 fp32 to tol 1e-6 (cap "
                                    "30000) + ADR to the stop rule (cap 100000)" % n,
                        "voxels": cells, "seed": SEED, "geometry_s": round(gen_s, 2)},
-            "mode": "streams: every solve's flow and transport loops as CUDA graphs on its own "
-                    "stream, all solves at once",
+            "mode": "tiles: one persistent launch per class of solves per step over a work "
+                    "list of 256-voxel tiles, K steps per CUDA graph, autotuned tiling",
             "plain": {"solves_per_hour": n / t_plain * 3600.0, "seconds": t_plain},
-            "tiles": {"solves_per_hour": n / t_tiles * 3600.0, "seconds": t_tiles,
-                      "identical_to_plain": all(_same(a, b) for a, b in zip(res_tiles, ref))},
+            "streams": {"solves_per_hour": n / t_streams * 3600.0, "seconds": t_streams,
+                        "identical_to_plain": all(_same(a, b) for a, b in zip(res_streams, ref))},
             "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": same,
             "failed": sum(1 for r in res if r.error is not None), "clocks": clk.summary()}
 
@@ -550,7 +558,7 @@ def main():
     ap.add_argument("--adr-sweep-steps", type=int, default=3000)
     ap.add_argument("--requests", type=int, default=48)
     ap.add_argument("--rate", type=float, default=20.0)
-    ap.add_argument("--serve-mode", default="tiles", choices=["streams", "tiles"])
+    ap.add_argument("--serve-mode", default="streams", choices=["streams", "tiles"])
     ap.add_argument("--flow-cap", type=int, default=2000000)
     args = ap.parse_args()
     if args.mode != "plain" and args.impl == "ours":
@@ -615,6 +623,7 @@ def main():
                 "detail": {"flow_ms": r["flow_ms"], "transport_ms": r["adr_ms"],
                            "flow_iters": r["iters"], "transport_steps": r["adr_steps"],
                            "voxels": r["ncell"], "pore_voxels": r["nfluid"],
+                           "e2e_ms": r["e2e_ms"], "e2e_split": r["e2e_split"],
                            "solves_per_hour": 3.6e6 / r["ms_per_step"] * world}}
         print(json.dumps(line))
     if dist is not None:

@@ -103,7 +103,7 @@ def pore_voxels(req):
 
 
 def serve(requests, arrivals, device=0, hbm_fraction=0.8, graph_steps=20, quiet=True,
-          budget_bytes=None, mode="tiles", flow_cap=2000000):
+          budget_bytes=None, mode="streams", flow_cap=2000000):
     """Serve `requests` arriving at host times `arrivals` (seconds after the
     start).  Admission is first-come first-served while the summed
     footprints stay within hbm_fraction of the device memory (or
@@ -114,9 +114,9 @@ def serve(requests, arrivals, device=0, hbm_fraction=0.8, graph_steps=20, quiet=
     that alone exceeds the cap is admitted when no flow is running.  Under
     overload this keeps the GPU full while finishing requests nearly in
     arrival order, instead of sharing the GPU among every queued request.
-    mode "tiles" advances the admitted solves with the batch engine's
-    tile-list kernels (Batch), "streams" as concurrent single-solve loops
-    (StreamBatch).  Returns a Served."""
+    mode "streams" runs the admitted solves as concurrent single-solve loops
+    (StreamBatch), "tiles" through the batch engine's tile-list kernels
+    (Batch).  Returns a Served."""
     order = np.argsort(np.asarray(arrivals, np.float64), kind="stable")
     pending = collections.deque((float(arrivals[i]), requests[i]) for i in order)
     if budget_bytes is None:
