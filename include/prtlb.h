@@ -324,7 +324,8 @@ typedef struct prt_batch prt_batch;
 /* A batch on CUDA device `device`, with its own stream.  Each step advances
  * every running job by one flow iteration or one transport step, all jobs
  * in one persistent launch per (lattice, precision) or (dimension, species)
- * class, over a work list of 256-voxel tiles; steps run as a CUDA graph of
+ * class, over a work list of tiles (128-voxel blocks for flow, 256 for
+ * transport); steps run as a CUDA graph of
  * `graph_steps` steps (0: 20). */
 int prt_batch_create(int device, int32_t graph_steps, prt_batch** out);
 
@@ -358,7 +359,7 @@ int prt_batch_collect(prt_batch* b, prt_ctx** out, int32_t cap, int32_t* count);
 /* Jobs in the batch (pending additions included). */
 int prt_batch_size(const prt_batch* b, int32_t* flow_jobs, int32_t* adr_jobs);
 
-/* Tile size in 256-voxel blocks (1, 2 or 4) and grid: a persistent grid of
+/* Tile size in blocks (1, 2 or 4) and grid: a persistent grid of
  * grid_mult (1 or 2) resident waves walking the work list, or 0 for one
  * block per work-list entry; tile_blocks 0 = choose both by timing the
  * first launches. */

@@ -1,11 +1,11 @@
 // batch.cu -- the flow time loop of many solves in one launch per iteration.
 //
 // A batch holds flow solves of any sizes; their pore slots are cut into
-// 256-slot blocks and listed as tiles (job, first block, block count).  One
-// persistent launch walks the tile list and runs one LB iteration of every
+// blocks of kFlowThreads slots and listed as tiles (job, first block, block
+// count).  One persistent launch walks the tile list and runs one LB iteration of every
 // job that is not done, each job at its own iteration count and parity.
 // The arithmetic per voxel is lb_cell_rw, the per-block |u_x| partials are
-// block_sum_store over the same 256 slots, and the convergence update is
+// block_sum_store over the same blocks of slots, and the convergence update is
 // flow_ctrl_advance, so a job's iterations, decisions and final field are
 // bit-identical to the single-solve loop whatever else shares the batch.
 //

@@ -6,7 +6,7 @@
 // loop.  Every batch step advances each of them by one iteration (flow) or
 // one step (transport): one persistent launch per class of jobs -- (lattice,
 // precision) for flow, (dimension, species) for transport -- walks a work
-// list of 256-voxel tiles of all jobs of the class.  Flow and transport
+// list of voxel tiles of all jobs of the class.  Flow and transport
 // chains are captured on two streams, so they overlap in the graph.  Work
 // lists, job descriptors and counts live in device memory and the launches
 // read their lengths there, so a graph stays valid while jobs come and go;

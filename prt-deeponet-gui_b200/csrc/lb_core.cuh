@@ -95,40 +95,40 @@ struct Pop<__half> {
 
 // Precision modes: storage type S, arithmetic R for the symmetric part and
 // RA for the momentum and the antisymmetric non-equilibrium part (a small
-// difference of two O(u) numbers), and the resident 256-thread blocks per SM
-// the register budget is cut for (single-solve and batched step kernels).
+// difference of two O(u) numbers), and the resident blocks of kFlowThreads
+// per SM the register budget is cut for (single-solve and batched steps).
 // `staged`: the arrived populations go to shared memory by cp.async, so no
 // register waits on a gather load (4- and 8-byte populations only).
 struct ModeF64 {  // the reference's arithmetic
     using S = double;
     using R = double;
     using RA = double;
-    static constexpr int min_blocks = 3;
-    static constexpr int batch_min_blocks = 3;
+    static constexpr int min_blocks = 6;
+    static constexpr int batch_min_blocks = 6;
     static constexpr bool staged = true;
 };
 struct ModeF32 {  // float32 populations, float32 collision
     using S = float;
     using R = float;
     using RA = float;
-    static constexpr int min_blocks = 5;
-    static constexpr int batch_min_blocks = 4;
+    static constexpr int min_blocks = 10;
+    static constexpr int batch_min_blocks = 8;
     static constexpr bool staged = true;
 };
 struct ModeF32D {  // float32 populations, float64 momentum
     using S = float;
     using R = float;
     using RA = double;
-    static constexpr int min_blocks = 5;
-    static constexpr int batch_min_blocks = 4;
+    static constexpr int min_blocks = 10;
+    static constexpr int batch_min_blocks = 8;
     static constexpr bool staged = true;
 };
 struct ModeF16 {  // scaled float16 populations, float32 collision
     using S = __half;
     using R = float;
     using RA = float;
-    static constexpr int min_blocks = 3;
-    static constexpr int batch_min_blocks = 3;
+    static constexpr int min_blocks = 6;
+    static constexpr int batch_min_blocks = 6;
     static constexpr bool staged = false;
 };
 
@@ -201,7 +201,9 @@ __device__ __forceinline__ void griddep_launch_dependents() {
 }
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
-constexpr int kFlowThreads = 256;
+// 128-thread blocks: at 64^3 (458 blocks of 256 for 148 SMs) finer blocks
+// balance the SMs better and cut an iteration from 6.25 to 5.73 us.
+constexpr int kFlowThreads = 128;
 
 // cp.async of one 4- or 8-byte population into this thread's shared slot.
 template <class S>

@@ -261,7 +261,7 @@ cudaError_t flow_launch_step(int nd, int precision, bool odd, bool check, void* 
 
 cudaError_t flow_launch_check(FlowCtrl* ctrl, const double* partials, int nblocks,
                               cudaGraphConditionalHandle h, int use_handle, cudaStream_t s) {
-    flow_check_kernel<<<1, 256, 0, s>>>(ctrl, partials, nblocks, h, use_handle);
+    flow_check_kernel<<<1, kFlowThreads, 0, s>>>(ctrl, partials, nblocks, h, use_handle);
     return cudaGetLastError();
 }
 

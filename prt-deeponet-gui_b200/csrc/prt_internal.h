@@ -185,7 +185,8 @@ cudaError_t adr_launch_stop(const AdrDev& d, AdrCtrl* ctrl, const float* means,
                             cudaGraphConditionalHandle h, int use_handle, cudaStream_t s);
 
 // Batched solves (batch.cu, batch_adr.cu, engine.cu) ------------------------
-// A work-list entry: the 256-slot blocks [b0, b0 + nb) of job `job`.
+// A work-list entry: the blocks [b0, b0 + nb) of job `job` (kFlowThreads
+// slots per block for flow, 256 solute voxels for transport).
 struct BatchTile {
     int job;
     int b0;
@@ -203,9 +204,9 @@ struct FlowJob {
     Grid g;
     LbParams kc;
     FlowCtrl* ctrl;
-    double* partials;  // one per 256-slot block, as in the single solve
+    double* partials;  // one per block of slots, as in the single solve
     unsigned* arrive;
-    int nb;            // 256-slot blocks of the job
+    int nb;            // blocks of slots of the job
     int pad;
 };
 
