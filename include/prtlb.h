@@ -271,8 +271,13 @@ int prt_adr_fetch_dev(prt_ctx* ctx, int32_t slot, float* d_out);
  * float32 pairwise summation order (what solve_adr's check uses). */
 int prt_adr_means(prt_ctx* ctx, int32_t slot, float* means);
 
-/* Release the transport state of the context. */
+/* Ends the transport state of the context.  Device buffers of up to
+ * 256 MiB each stay with the context for its next transport run (so
+ * back-to-back solves skip the allocator); larger ones are freed. */
 int prt_adr_end(prt_ctx* ctx);
+
+/* Frees every transport buffer of the context (prt_destroy does too). */
+int prt_adr_release(prt_ctx* ctx);
 
 /* ------------------------------------------------------------------------
  * Batched and served solves.  No counterpart in the reference, which runs

@@ -119,7 +119,10 @@ struct ModeF32D {  // float32 populations, float64 momentum
     using S = float;
     using R = float;
     using RA = double;
-    static constexpr int min_blocks = 10;
+    // 64 registers: at 48 (10 blocks) the step kernel spills, and 64^3
+    // (917 blocks) still fits one wave at 8 blocks per SM (5.67 -> 5.41 us
+    // per iteration; 128^3 unchanged)
+    static constexpr int min_blocks = 8;
     static constexpr int batch_min_blocks = 8;
     static constexpr bool staged = true;
 };
@@ -149,6 +152,15 @@ __device__ __forceinline__ void upstream_slots(const FlowMap& fm, const Grid& g,
         const int a = 1 - L::c(i, 0), b = 1 - L::c(i, 1), c = 1 - L::c(i, 2);
         src[i] = fm.imap[(X[a] * g.ny + Y[b]) * g.nz + Z[c]];
     }
+}
+
+// The same slots from the upstream-slot table fm.nbr (coalesced: entry i-1
+// of every slot is one contiguous row).
+template <class L>
+__device__ __forceinline__ void upstream_slots_table(const FlowMap& fm, int k, int (&src)[L::Q]) {
+    src[0] = k;
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) src[i] = __ldg(fm.nbr + (i - 1) * fm.nf + k);
 }
 
 // Gather the arrived populations of pore voxel number k (see the file

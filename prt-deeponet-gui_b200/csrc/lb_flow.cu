@@ -38,7 +38,10 @@ __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
     // the pore maps never change during a solve: the upstream slots are
     // looked up while the previous iteration may still be running
     int src[L::Q];
-    if (k < fm.nf) upstream_slots<L>(fm, g, k, src);
+    if (k < fm.nf) {
+        if (fm.nbr) upstream_slots_table<L>(fm, k, src);
+        else upstream_slots<L>(fm, g, k, src);
+    }
     griddep_wait();
     const long long it = ctrl->it_base + kstep;
     if (ctrl->done || it >= ctrl->nit) return;  // uniform over the grid
@@ -196,6 +199,17 @@ __global__ void imap_scatter_kernel(int* __restrict__ cells, int nf, int* __rest
     cells[k] = (int)(((unsigned)x << xs) | ((unsigned)y << ys) | (unsigned)z);
 }
 
+// The upstream-slot table: nbr[(i - 1) * nf + k] = upstream slot i of slot k.
+template <class L>
+__global__ void nbr_fill_kernel(FlowMap fm, Grid g, int* __restrict__ nbr) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= fm.nf) return;
+    int src[L::Q];
+    upstream_slots<L>(fm, g, k, src);
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) nbr[(i - 1) * fm.nf + k] = src[i];
+}
+
 // -------------------------------------------------------------------------
 // launchers
 // -------------------------------------------------------------------------
@@ -291,6 +305,14 @@ cudaError_t flow_launch_imap(int* cells, int nf, int* imap, const Grid& g, int y
                              cudaStream_t s) {
     if (nf <= 0) return cudaSuccess;
     imap_scatter_kernel<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(cells, nf, imap, g, ys, xs);
+    return cudaGetLastError();
+}
+
+cudaError_t flow_launch_nbr(int nd, const FlowMap& fm, const Grid& g, int* nbr, cudaStream_t s) {
+    if (fm.nf <= 0) return cudaSuccess;
+    const unsigned nb = (unsigned)((fm.nf + 255) / 256);
+    if (nd == 3) nbr_fill_kernel<D3Q19><<<nb, 256, 0, s>>>(fm, g, nbr);
+    else nbr_fill_kernel<D2Q9><<<nb, 256, 0, s>>>(fm, g, nbr);
     return cudaGetLastError();
 }
 

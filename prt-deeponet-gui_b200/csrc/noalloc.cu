@@ -204,6 +204,7 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
     fm.nf = (int)nfluid;
     fm.cells = cells;
     fm.imap = imap;
+    fm.nbr = nullptr;
     const int nb = std::max(flow_blocks(nfluid), 1);
     NCK(cudaMemsetAsync(f, 0, (size_t)2 * Q * nfluid * es, s));
     NCK(cudaMemsetAsync(d_vel_out, 0, (size_t)3 * g.n * sizeof(float), s));

@@ -105,13 +105,29 @@ struct PairTree {
 // voxel in C order, whose coordinates are packed in cells[k] as
 // x << xs | y << ys | z (so a kernel finds its neighbours with shifts and
 // masks instead of divisions); imap[voxel] is the slot of a pore voxel, -1
-// for rock.
+// for rock.  nbr, when not null, is the table of upstream slots
+// nbr[(i - 1) * nf + k] = slot of voxel k - e_i or -1 (i = 1 .. Q-1): the
+// step kernel then reads them in one coalesced pass instead of the packed
+// cell and imap lookups (one dependent load fewer).  Set up for solves whose
+// lattices and table fit in half the L2 cache, where the latency of the
+// lookups, not the bytes of the table, bounds an iteration.
 struct FlowMap {
     int nf;
     const int* cells;
     const int* imap;
     int ys, xs;  // bit offsets of y and x in a packed cell
+    const int* nbr;
 };
+
+// Bytes of the upstream-slot table of nf pore voxels (Q-1 ints each).
+inline long long flow_nbr_bytes(int q, long long nf) { return (long long)(q - 1) * nf * 4; }
+
+// Whether a solve with nf pore voxels and populations of es bytes gets the
+// upstream-slot table on a device with l2_bytes of L2: when the two
+// lattices and the table fit in half of it.
+inline bool flow_use_nbr(int q, long long nf, long long es, long long l2_bytes) {
+    return nf > 0 && 2 * q * nf * es + flow_nbr_bytes(q, nf) <= l2_bytes / 2;
+}
 
 // Bits that hold the values 0 .. n-1.
 __host__ __device__ inline int coord_bits(int n) {
@@ -146,6 +162,9 @@ cudaError_t flow_launch_flags(const uint8_t* mat, long long n, int pore, uint8_t
 // packed coordinates of fm (imap must hold -1 everywhere before).
 cudaError_t flow_launch_imap(int* cells, int nf, int* imap, const Grid& g, int ys, int xs,
                              cudaStream_t s);
+// The upstream-slot table of fm (cells and imap ready) into nbr,
+// flow_nbr_bytes(Q, fm.nf) bytes.
+cudaError_t flow_launch_nbr(int nd, const FlowMap& fm, const Grid& g, int* nbr, cudaStream_t s);
 cudaError_t flow_launch_final_reduce(const double* partials, int nblocks, double* out,
                                      cudaStream_t s);
 int flow_blocks(long long n);

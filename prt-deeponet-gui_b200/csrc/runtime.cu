@@ -2,6 +2,7 @@
 // buffers, and the two time loops run as CUDA graphs with a device-side
 // while-condition, so a whole flow solve or transport solve is one graph
 // launch and the host waits once.
+#include <cstdlib>
 #include <new>
 
 #include "runtime_internal.h"
@@ -37,6 +38,9 @@ extern "C" int prt_create(int device, prt_ctx** out) {
     e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    int l2 = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device);
+    c->l2_bytes = l2;
     if (e != cudaSuccess) {
         g_create_error = std::string("cuda init failed: ") + cudaGetErrorString(e);
         delete c;
@@ -54,7 +58,7 @@ extern "C" void prt_destroy(prt_ctx* c) {
     c->adr.release();
     FlowState& f = c->flow;
     DevBuf* all[] = {&f.f,    &f.fluid, &f.partials, &f.ctrl, &f.out5, &f.count,
-                     &f.mat,  &f.vel,   &f.flag,     &f.cnt,  &f.cells};
+                     &f.mat,  &f.vel,   &f.flag,     &f.cnt,  &f.cells, &f.nbr};
     for (DevBuf* b : all) b->release();
     f.graph.release();
     for (int i = 0; i < 4; ++i)
@@ -96,6 +100,20 @@ extern "C" size_t prt_sizeof(int which) {
 // ===========================================================================
 // flow
 // ===========================================================================
+// Transport buffers up to this size outlive prt_adr_end on their context.
+constexpr size_t kAdrKeepBytes = size_t(256) << 20;
+
+// The upstream-slot table: by the working set against the L2 cache
+// (flow_use_nbr), or always / never with PRT_NBR_TABLE=1 / 0.  Both ways
+// give the same slots, so the fields are bit-identical either way.
+static bool nbr_table_wanted(int q, long long nf, long long es, long long l2_bytes) {
+    if (nf <= 0) return false;
+    const char* v = std::getenv("PRT_NBR_TABLE");
+    if (v && v[0] == '1') return true;
+    if (v && v[0] == '0') return false;
+    return flow_use_nbr(q, nf, es, l2_bytes);
+}
+
 // Flow solve in three parts, so the batched engine can run many set-up
 // solves through one time loop: set-up (buffers, pore-only layout, control
 // block, constants), the time loop, and the final field with its reductions.
@@ -149,6 +167,13 @@ int prt::flow_setup(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p
     F.fm.nf = (int)nfluid;
     F.fm.cells = F.cells.as<int>();
     F.fm.imap = F.fluid.as<int>();
+    F.fm.nbr = nullptr;
+    if (nbr_table_wanted(Q, nfluid, (long long)es, ctx->l2_bytes)) {
+        CK(F.nbr.ensure((size_t)flow_nbr_bytes(Q, nfluid)));
+        CK(flow_launch_nbr(p->nd, F.fm, g, F.nbr.as<int>(), s));
+        ctx->launches += 1;
+        F.fm.nbr = F.nbr.as<int>();
+    }
     F.nb = std::max(flow_blocks(nfluid), 1);
     CK(F.f.ensure((size_t)2 * Q * std::max(nfluid, 1ll) * es));  // two lattices
     CK(F.partials.ensure((size_t)F.nb * 5 * sizeof(double)));
@@ -246,7 +271,7 @@ static int flow_graph(prt_ctx* ctx) {
     key.force = p.force; key.tau = p.tau; key.magic = p.magic; key.nit = p.nit;
     key.tol = p.tol; key.f = F.f.p;
     key.aux[0] = F.fluid.p; key.aux[1] = F.partials.p; key.aux[2] = F.ctrl.p;
-    key.aux[3] = F.cells.p; key.nf = F.nfluid;
+    key.aux[3] = F.cells.p; key.aux[4] = (void*)F.fm.nbr; key.nf = F.nfluid;
     if (!F.graph.exec || !(key == F.key)) {
         CK(build_while_graph(ctx->stream,
                              F.graph, [&](cudaGraphConditionalHandle h, int use) {
@@ -827,6 +852,14 @@ extern "C" int prt_adr_means(prt_ctx* ctx, int32_t slot, float* means) {
 }
 
 extern "C" int prt_adr_end(prt_ctx* ctx) {
+    if (!ctx) return PRT_E_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->adr.release(kAdrKeepBytes);
+    return PRT_OK;
+}
+
+extern "C" int prt_adr_release(prt_ctx* ctx) {
     if (!ctx) return PRT_E_INVALID;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);

@@ -62,24 +62,25 @@ struct FlowKey {
     long long nit = -1;
     double tol = 0;
     void* f = nullptr;
-    void* aux[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* aux[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     long long nf = -1;  // pore voxels: launch sizes and the lattice stride are baked in
     bool operator==(const FlowKey& o) const {
         return nd == o.nd && precision == o.precision && every == o.every && g.nx == o.g.nx &&
                g.ny == o.g.ny && g.nz == o.g.nz && force == o.force && tau == o.tau &&
                magic == o.magic && nit == o.nit && tol == o.tol && f == o.f && aux[0] == o.aux[0] &&
-               aux[1] == o.aux[1] && aux[2] == o.aux[2] && aux[3] == o.aux[3] && nf == o.nf;
+               aux[1] == o.aux[1] && aux[2] == o.aux[2] && aux[3] == o.aux[3] &&
+               aux[4] == o.aux[4] && nf == o.nf;
     }
 };
 
 struct FlowState {
-    DevBuf f, fluid, partials, ctrl, out5, count, mat, vel, flag, cnt, cells;
+    DevBuf f, fluid, partials, ctrl, out5, count, mat, vel, flag, cnt, cells, nbr;
     GraphHolder graph;
     FlowKey key;
     // the solve set up by flow_setup
     prt_flow_params p{};
     Grid g{0, 0, 0, 0};
-    FlowMap fm{0, nullptr, nullptr};
+    FlowMap fm{0, nullptr, nullptr, 0, 0, nullptr};
     LbParams kc{};
     int nb = 1;
     long long nfluid = 0;
@@ -88,7 +89,7 @@ struct FlowState {
     float* d_vel = nullptr;          // its output field (borrowed)
     bool field_ready = false;        // d_vel holds the final field
     void release_lattices() {
-        DevBuf* all[] = {&f, &fluid, &partials, &count, &flag, &cnt, &cells};
+        DevBuf* all[] = {&f, &fluid, &partials, &count, &flag, &cnt, &cells, &nbr};
         for (DevBuf* b : all) b->release();
         graph.release();
         key = FlowKey();
@@ -114,12 +115,17 @@ struct AdrState {
     std::vector<int> slot_of_index;     // ladder index -> slot
     int nslots = 0;
     GraphHolder graph;
-    void release() {
+    // Ends the transport state.  Device buffers of at most keep_bytes stay
+    // with the context for its next run (every run sizes them with ensure()
+    // and initialises what it reads), so back-to-back solves on one context
+    // do not pay cudaFree / cudaMalloc each time; larger ones are freed.
+    void release(size_t keep_bytes = 0) {
         DevBuf* all[] = {&mat, &vel, &flags, &mflag, &face[0], &face[1], &face[2], &buf[0], &buf[1],
                          &ladder, &slot_of_step, &idx, &cnt, &total, &tree_leaf_start,
                          &tree_leaf_len, &tree_inner_l, &tree_inner_r, &tree_level_off, &tree_vals,
                          &means, &src_slot, &ctrl, &log, &tmp, &vstats};
-        for (DevBuf* b : all) b->release();
+        for (DevBuf* b : all)
+            if (b->bytes > keep_bytes) b->release();
         staged = false;
         graph.release();
         keep_steps.clear();
@@ -143,6 +149,7 @@ struct prt_ctx {
     bool adr_armed = false;   // transport run set up, its time loop not finished
     prt_batch* batch = nullptr;  // the batch holding this context, if any
     int running = 0;             // a loop enqueued by prt_*_launch: 1 flow, 2 transport
+    long long l2_bytes = 0;      // the device's L2 cache
 };
 
 namespace prt {

@@ -45,6 +45,11 @@ def footprint(req):
     es = {"fp64": 8, "fp32": 4, "fp32f": 4, "fp16": 2}[req.flow["precision"]]
     common = n * (1 + 12)
     flow = 2 * q * nf * es + 4 * nf + 4 * n + n + 5 * 8 * (nf // 256 + 1)
+    # the upstream-slot table of solves that fit in half the L2 cache,
+    # counted up to an L2 of 256 MiB (an upper bound of the devices run on)
+    table = 4 * (q - 1) * nf
+    if 2 * q * nf * es + table <= (128 << 20):
+        flow += table
     adr = 0
     if req.adr is not None:
         a = req.adr

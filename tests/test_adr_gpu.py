@@ -87,3 +87,30 @@ def test_progress_callback_exception_propagates():
     with contextlib.redirect_stdout(io.StringIO()):
         out, _ = solve_adr(g, v, pe=30.0, da=1.0, n_t=3, n_species=1, steps=50)
     assert np.isfinite(out).all()
+
+
+def test_buffers_kept_between_runs_hold_no_stale_values():
+    """prt_adr_end keeps the transport buffers on the context for its next
+    run.  Runs on one context, largest grid first, then smaller 3D and 2D
+    grids with other porosities, match their golden runs bit for bit: every
+    run initialises what it reads, so nothing of an earlier run leaks in
+    (rock voxels included).  prt_adr_release then frees them and the
+    context still works."""
+    from prtlb_gpu import _lib, solve_adr
+    names = sorted(ADR32, key=lambda n: -load_golden(n)["mat"].size)
+    ctx = _lib.Context(0)
+    try:
+        for name in names[:4] + names[-2:]:
+            z = load_golden(name)
+            kw = adr_kwargs(z, name)
+            with contextlib.redirect_stdout(io.StringIO()):
+                out, tn = solve_adr(z["mat"], z["vel"], ctx=ctx, **kw)
+            assert np.array_equal(out, z["out"]), name
+            assert np.array_equal(tn, z["t_norm"]), name
+        ctx.check(_lib.lib().prt_adr_release(ctx.handle))
+        z = load_golden(names[0])
+        with contextlib.redirect_stdout(io.StringIO()):
+            out, _ = solve_adr(z["mat"], z["vel"], ctx=ctx, **adr_kwargs(z, names[0]))
+        assert np.array_equal(out, z["out"])
+    finally:
+        ctx.close()

@@ -144,3 +144,26 @@ def test_programmatic_dependent_launch_gives_the_same_field(monkeypatch):
         monkeypatch.setenv("PRT_PDL", "1")
         got = stokes_d3q19(g, nit=400, tol=0.0, precision="fp32")
     assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp16"])
+def test_upstream_slot_table_gives_the_same_field(monkeypatch, precision):
+    """Small solves read their upstream slots from a precomputed table, large
+    ones look them up through the packed cells and the voxel map
+    (PRT_NBR_TABLE=1 / 0 force either way): the same slots, so the same
+    field bit for bit and the same stop iteration."""
+    from prtlb_gpu import sphere_pack_3d, stokes_d3q19, stokes_d2q9
+    from prtlb_gpu.geometry import disk_pack_2d
+    g3 = sphere_pack_3d(24, 0.45, 1)
+    g2 = disk_pack_2d(40, 0.5, 1)
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("PRT_NBR_TABLE", mode)
+        i3 = {}
+        with contextlib.redirect_stdout(io.StringIO()):
+            v3 = stokes_d3q19(g3, nit=600, tol=1e-9, precision=precision, info=i3)
+            v2 = stokes_d2q9(g2, nit=500, tol=0.0, precision=precision)
+        out[mode] = (v3, i3["flow_iters"], v2)
+    assert np.array_equal(out["0"][0], out["1"][0])
+    assert out["0"][1] == out["1"][1]
+    assert np.array_equal(out["0"][2], out["1"][2])
