@@ -13,16 +13,28 @@ namespace prt {
 // numpy's elementwise semantics ---------------------------------------------
 __device__ __forceinline__ float np_min(float a, float b) { return (a <= b || a != a) ? a : b; }
 __device__ __forceinline__ float np_max(float a, float b) { return (a >= b || a != a) ? a : b; }
-__device__ __forceinline__ float np_sign(float a) {
-    return a > 0.f ? 1.f : (a < 0.f ? -1.f : (a != a ? a : 0.f));
+
+// min of two values that is NaN when either is (as np_min's value; the NaN
+// may carry another payload).
+__device__ __forceinline__ float min_nan(float a, float b) {
+    float r;
+    asm("min.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
 }
 
 // _muscl (prtlb_3d.py:650-705): up + 1/2 minmod(down - up, up - upup), the
-// minmod written as 1/2 (sgn a + sgn b) min(|a|, |b|).
+// minmod written as 1/2 (sgn a + sgn b) min(|a|, |b|).  The signs are taken
+// from the sign bits (copysign(1, d)), which differs from numpy's sign()
+// only at d = +-0; there min(|a|, |b|) = 0, the slope is a zero of either
+// sign, and up + 1/2 slope is up exactly unless up is -0.  No concentration
+// is ever -0 (states start at +0 or above, a sum is -0 only of two -0
+// operands, and the clip keeps its operand), so the result is numpy's bit
+// for bit; NaN reaches it through the min.
 __device__ __forceinline__ float muscl(float up, float upup, float down) {
     const float d1 = down - up;
     const float d2 = up - upup;
-    const float slope = (0.5f * (np_sign(d1) + np_sign(d2))) * np_min(fabsf(d1), fabsf(d2));
+    const float slope =
+        (0.5f * (copysignf(1.f, d1) + copysignf(1.f, d2))) * min_nan(fabsf(d1), fabsf(d2));
     return up + 0.5f * slope;
 }
 
@@ -55,6 +67,19 @@ __device__ __forceinline__ VoxelPos voxel_pos(int c, const Grid& g) {
     t /= (unsigned)g.nz;
     v.p[1] = (int)(t % (unsigned)g.ny);
     v.p[0] = (int)(t / (unsigned)g.ny);
+    return v;
+}
+
+// The same with the run's precomputed divisors (c < 2^31).
+__device__ __forceinline__ VoxelPos voxel_pos(int c, const FastDiv& dz, const FastDiv& dy) {
+    VoxelPos v;
+    v.c = c;
+    const unsigned t = (unsigned)c;
+    const unsigned q = fast_div(t, dz);
+    v.p[2] = (int)(t - q * dz.d);
+    const unsigned x = fast_div(q, dy);
+    v.p[1] = (int)(q - x * dy.d);
+    v.p[0] = (int)x;
     return v;
 }
 
@@ -137,8 +162,12 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
         const float DH = oH ? (nh == 0 ? dj[0] : (nh == 1 ? dj[1] : dj[2])) : 0.f;
         // out += D_hi (C+1 - C) + D_lo (C-1 - C)
         out = out + (DH * (Cp1 - Cc) + DL * (Cm1 - Cc));
-        const float fh = (uH >= 0.f) ? muscl(Cc, Cm1, Cp1) : muscl(Cp1, Cp2, Cc);
-        const float flo = (uL >= 0.f) ? muscl(Cm1, Cm2, Cc) : muscl(Cc, Cp1, Cm1);
+        // upwind face values: the stencil is chosen first and limited once
+        // (the same function of the same three values as choosing between
+        // the two limited candidates)
+        const bool rH = uH >= 0.f, rL = uL >= 0.f;
+        const float fh = muscl(rH ? Cc : Cp1, rH ? Cm1 : Cp2, rH ? Cp1 : Cc);
+        const float flo = muscl(rL ? Cm1 : Cc, rL ? Cm2 : Cp1, rL ? Cc : Cm1);
         // out -= u_hi f_hi - u_lo f_lo
         out = out - (uH * fh - uL * flo);
         divu = divu + (uH - uL);
@@ -220,7 +249,7 @@ __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params&
     const int N = (int)d.g.n;
     const float* __restrict__ Cin = d.buf[(n - 1) & 1];
     float* __restrict__ Cout = d.buf[n & 1];
-    const VoxelPos v = voxel_pos(c, d.g);
+    const VoxelPos v = voxel_pos(c, d.div_z, d.div_y);
     const bool x0 = fl & F_X0;
     float C[NS];
 #pragma unroll

@@ -17,6 +17,32 @@ struct Grid {
     long long n;  // nx*ny*nz
 };
 
+// Division by a divisor fixed for a whole run as one high multiply, one add
+// and one shift: the round-up method of Granlund and Montgomery ("Division
+// by invariant integers using multiplication", PLDI 1994) with a 33-bit
+// multiplier 2^32 + m, s = ceil(log2 d).  Exact for 0 <= t < 2^31 (then
+// the add cannot carry out of 32 bits).
+struct FastDiv {
+    unsigned d, m;
+    int s;
+};
+
+inline FastDiv make_fastdiv(unsigned d) {
+    FastDiv f;
+    f.d = d;
+    f.s = 0;
+    while (f.s < 31 && (1u << f.s) < d) ++f.s;
+    const unsigned long long two32 = 1ull << 32;
+    f.m = (unsigned)((two32 * ((1ull << f.s) - d)) / d + 1);
+    return f;
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ unsigned fast_div(unsigned t, const FastDiv& f) {
+    return (__umulhi(t, f.m) + t) >> f.s;
+}
+#endif
+
 // Device-side state of FlowConvergence (prtlb_3d.py:168-252) for one solve.
 struct FlowCtrl {
     long long it_base;  // iterations completed before the current chunk
@@ -179,6 +205,7 @@ void set_noctx_error(const char* msg);
 // Kernel launchers (adr.cu) -------------------------------------------------
 struct AdrDev {
     Grid g;
+    FastDiv div_z, div_y;  // by nz and by ny (coordinates of a voxel index)
     int nd;
     int ns;
     const uint32_t* flags;

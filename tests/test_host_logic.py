@@ -104,3 +104,37 @@ def test_native_pack_loop_matches_numpy_loop():
         g1 = random_pack(shp, phi, a, b, seed=sd, overlap_after=300)
         g2 = random_pack(shp, phi, a, b, seed=sd, overlap_after=300, native=False)
         assert np.array_equal(g1, g2), shp
+
+
+def _fastdiv(d):
+    """make_fastdiv of csrc/prt_internal.h, restated: s = ceil(log2 d),
+    m = floor(2^32 (2^s - d) / d) + 1."""
+    s = 0
+    while s < 31 and (1 << s) < d:
+        s += 1
+    m = ((1 << 32) * ((1 << s) - d)) // d + 1
+    assert 0 < m < (1 << 32)
+    return m, s
+
+
+def test_multiply_shift_division_is_exact_below_2_pow_31():
+    """The transport step finds voxel coordinates with fast_div (high
+    multiply, add, shift).  Checked here against integer division for every
+    divisor up to 4096 and the powers of two and their neighbours above it,
+    on numerators spread over [0, 2^31) with the multiples of d and their
+    neighbours, and the ends of the range."""
+    rng = np.random.default_rng(0)
+    divisors = list(range(1, 4097)) + [x + o for k in range(12, 31)
+                                        for x in (1 << k,) for o in (-1, 0, 1)]
+    top = (1 << 31) - 1
+    for d in divisors:
+        m, s = _fastdiv(d)
+        ks = np.concatenate([np.arange(0, 4), [top // d - 1, top // d],
+                             rng.integers(0, top // d + 1, 200)]).astype(np.int64)
+        near = (ks[:, None] * d + np.arange(-1, 2)[None, :]).ravel()
+        t = np.concatenate([rng.integers(0, top, 4000, dtype=np.int64), near,
+                            np.arange(0, min(3 * d + 3, 20000), dtype=np.int64),
+                            np.array([top, top - 1], np.int64)])
+        t = t[(t >= 0) & (t <= top)].astype(np.uint64)
+        q = (((t * np.uint64(m)) >> np.uint64(32)) + t) >> np.uint64(s)
+        assert np.array_equal(q, t // np.uint64(d)), d
