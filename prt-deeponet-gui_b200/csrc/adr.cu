@@ -20,7 +20,7 @@ constexpr int kAdrThreads = 128;
 
 // One transport step n = n_base + kstep + 1 over every solute voxel (one
 // thread each; rock voxels are never touched and stay 0 in every buffer).
-template <int ND, int NS>
+template <int ND, int NS, bool BF>
 __global__ void __launch_bounds__(kAdrThreads) adr_step_kernel(AdrDev d, prt_adr_params p,
                                                                const AdrCtrl* __restrict__ ctrl,
                                                                int kstep) {
@@ -28,7 +28,7 @@ __global__ void __launch_bounds__(kAdrThreads) adr_step_kernel(AdrDev d, prt_adr
     if (ctrl->done || n > ctrl->limit) return;  // uniform over the grid
     const long long kk = (long long)blockIdx.x * kAdrThreads + threadIdx.x;
     if (kk >= d.nm) return;
-    adr_voxel<ND, NS>(d, p, n, kk);
+    adr_voxel<ND, NS, BF>(d, p, n, kk);
 }
 
 // ---------------------------------------------------------------------------
@@ -239,7 +239,8 @@ static cudaError_t step_t(const AdrDev& d, const prt_adr_params& p, AdrCtrl* ctr
                           cudaStream_t s) {
     if (d.nm <= 0) return cudaSuccess;
     const unsigned nb = (unsigned)((d.nm + kAdrThreads - 1) / kAdrThreads);
-    adr_step_kernel<ND, NS><<<nb, kAdrThreads, 0, s>>>(d, p, ctrl, k);
+    if (d.has_bf) adr_step_kernel<ND, NS, true><<<nb, kAdrThreads, 0, s>>>(d, p, ctrl, k);
+    else adr_step_kernel<ND, NS, false><<<nb, kAdrThreads, 0, s>>>(d, p, ctrl, k);
     return cudaGetLastError();
 }
 

@@ -118,8 +118,10 @@ __device__ __forceinline__ float ld_c(const float* __restrict__ Cj, int c, int x
     return (pin && x == 0) ? feed : v;
 }
 
-// transport() of one chemical at one voxel (prtlb_3d.py:1182-1208).
-template <int ND>
+// transport() of one chemical at one voxel (prtlb_3d.py:1182-1208).  BF:
+// the run has biofilm; without it no voxel carries a biofilm flag, every
+// face takes the pore diffusivity, and the biofilm count is not formed.
+template <int ND, bool BF>
 __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, const Grid& g,
                                                const VoxelPos& v, uint32_t fl,
                                                const float* const* __restrict__ face, float Cc,
@@ -153,13 +155,19 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
         const float Cp1 = oH ? vp1 : Cc;
         const float Cm2 = fL ? vm2 : Cm1;
         const float Cp2 = fH ? vp2 : Cp1;
-        const int bf = (fl & F_BF) ? 1 : 0;
-        // face diffusivity by the biofilm count of its two voxels (0, 1, 2);
-        // selected, not indexed, so the table stays in registers
-        const int nl = bf + ((fl & f_nbf_lo(a)) ? 1 : 0);
-        const int nh = bf + ((fl & f_nbf_hi(a)) ? 1 : 0);
-        const float DL = oL ? (nl == 0 ? dj[0] : (nl == 1 ? dj[1] : dj[2])) : 0.f;
-        const float DH = oH ? (nh == 0 ? dj[0] : (nh == 1 ? dj[1] : dj[2])) : 0.f;
+        float DL, DH;
+        if constexpr (BF) {
+            const int bf = (fl & F_BF) ? 1 : 0;
+            // face diffusivity by the biofilm count of its two voxels (0, 1,
+            // 2); selected, not indexed, so the table stays in registers
+            const int nl = bf + ((fl & f_nbf_lo(a)) ? 1 : 0);
+            const int nh = bf + ((fl & f_nbf_hi(a)) ? 1 : 0);
+            DL = oL ? (nl == 0 ? dj[0] : (nl == 1 ? dj[1] : dj[2])) : 0.f;
+            DH = oH ? (nh == 0 ? dj[0] : (nh == 1 ? dj[1] : dj[2])) : 0.f;
+        } else {
+            DL = oL ? dj[0] : 0.f;
+            DH = oH ? dj[0] : 0.f;
+        }
         // out += D_hi (C+1 - C) + D_lo (C-1 - C)
         out = out + (DH * (Cp1 - Cc) + DL * (Cm1 - Cc));
         // upwind face values: the stencil is chosen first and limited once
@@ -241,7 +249,7 @@ __device__ __forceinline__ void reaction(const float (&C)[NS], float surf,
 // One transport step of solute voxel number kk (compacted C-order list) at
 // step n: reads the state after step n-1 from buf[(n-1)&1], writes the state
 // after step n to buf[n&1] and, when n is a snapshot step, to its ladder slot.
-template <int ND, int NS>
+template <int ND, int NS, bool BF = true>
 __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params& p, long long n,
                                           long long kk) {
     const int c = d.idx[kk];
@@ -264,7 +272,7 @@ __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params&
         if ((p.moving_mask >> j) & 1u) {
             const bool pin = (p.pinned_mask >> j) & 1u;
             const float dj[3] = {p.dface[j][0], p.dface[j][1], p.dface[j][2]};
-            T[j] = transport_one<ND>(Cin + j * N, d.g, v, fl, d.face, C[j], pin,
+            T[j] = transport_one<ND, BF>(Cin + j * N, d.g, v, fl, d.face, C[j], pin,
                                      p.feed[j], dj);
         }
     }

@@ -208,6 +208,7 @@ struct AdrDev {
     FastDiv div_z, div_y;  // by nz and by ny (coordinates of a voxel index)
     int nd;
     int ns;
+    int has_bf;  // the run has a biofilm material code (else no biofilm flag is set)
     const uint32_t* flags;
     const float* face[3];
     float* buf[2];

@@ -426,6 +426,7 @@ extern "C" int prt_adr_stage_dev(prt_ctx* ctx, const uint8_t* d_mat, const float
     A.d.g = g;
     A.d.div_z = make_fastdiv((unsigned)g.nz);
     A.d.div_y = make_fastdiv((unsigned)g.ny);
+    A.d.has_bf = geom->biofilm_code >= 0 ? 1 : 0;
     A.d.nd = geom->nd;
     CK(A.flags.ensure((size_t)N * 4));
     CK(A.mflag.ensure((size_t)N));
