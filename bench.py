@@ -64,8 +64,10 @@ FORCE, TAU, FLOW_TOL, FLOW_NIT = 2e-6, 0.8, 1e-6, 30000
 ADR_STEPS = None  # None: run to the reference's stop rule
 # DRAM bytes (read + write) of one lb_step_kernel launch from an ncu capture
 # (cache flushed before the launch), by grid edge: profiles/
-# lb_step_kernel_plain3d_64.md and lb_step_kernel_sphere128.md
-TRAFFIC_PER_LAUNCH = {64: 18238464, 128: 178001408}
+# lb_step_kernel_plain3d_64.md and lb_step_kernel_sphere128.md.  At 64^3
+# they include the upstream-slot table (72 B per pore voxel, 8.4 MB), which
+# the solve reads instead of the voxel map because its working set fits in L2.
+TRAFFIC_PER_LAUNCH = {64: 25157632, 128: 176652032}
 PE, DA, KS, N_T = 10.0, 1.0, 0.5, 5
 METRIC = "D3Q19 TRT+ADR GLUPS"
 UNIT = "GLUPS"
@@ -293,8 +295,10 @@ def run_ours(args, rank, world, torch, dist):
             "frac": round(achieved / peak, 4), "peak_kind": kind,
             "bytes_per_launch": lb_bytes, "traffic": TRAFFIC_PER_LAUNCH.get(EDGE),
             "note": "algorithmic bytes = 152 B per pore voxel (19 float32 read + written) + "
-                    "4 B neighbour mask per voxel; per-launch time = flow loop events / "
-                    "iterations (includes graph node gaps and the convergence check)"}
+                    "4 B voxel map per voxel; per-launch time = flow loop events / "
+                    "iterations (includes graph node gaps and the convergence check); at "
+                    "this size the kernel reads a 72 B per pore voxel upstream-slot table "
+                    "from L2 instead of the map (traffic is a cold-cache capture)"}
     res = {"ms_per_step": total_ms / args.steps, "value": value, "e2e": e2e_value,
            "h2d": h2d, "d2h": d2h, "launches": launches, "roof": roof, "clocks": clk.summary(),
            "flow_ms": fl_ms, "adr_ms": ad_ms, "iters": iters[0], "adr_steps": nsteps[0],
