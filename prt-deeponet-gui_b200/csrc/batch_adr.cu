@@ -36,9 +36,15 @@ __global__ void __launch_bounds__(kBatchAdrThreads)
         if (ctrl->done) continue;
         const long long n = ctrl->n_base + 1;
         if (n > ctrl->limit) continue;
+        // a job without biofilm takes the voxel step without the biofilm
+        // selects (uniform over the block: J is the tile's job)
+        const bool bf = J.d.has_bf != 0;
         for (int b = tl.b0; b < tl.b0 + tl.nb; ++b) {
             const long long kk = (long long)b * kBatchAdrThreads + threadIdx.x;
-            if (kk < J.d.nm) adr_voxel<ND, NS>(J.d, J.p, n, kk);
+            if (kk < J.d.nm) {
+                if (bf) adr_voxel<ND, NS, true>(J.d, J.p, n, kk);
+                else adr_voxel<ND, NS, false>(J.d, J.p, n, kk);
+            }
         }
     }
 }

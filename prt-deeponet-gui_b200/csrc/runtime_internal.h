@@ -64,12 +64,13 @@ struct FlowKey {
     void* f = nullptr;
     void* aux[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     long long nf = -1;  // pore voxels: launch sizes and the lattice stride are baked in
+    int pdl = 0;        // step kernels captured with programmatic dependent launch
     bool operator==(const FlowKey& o) const {
         return nd == o.nd && precision == o.precision && every == o.every && g.nx == o.g.nx &&
                g.ny == o.g.ny && g.nz == o.g.nz && force == o.force && tau == o.tau &&
                magic == o.magic && nit == o.nit && tol == o.tol && f == o.f && aux[0] == o.aux[0] &&
                aux[1] == o.aux[1] && aux[2] == o.aux[2] && aux[3] == o.aux[3] &&
-               aux[4] == o.aux[4] && nf == o.nf;
+               aux[4] == o.aux[4] && nf == o.nf && pdl == o.pdl;
     }
 };
 
