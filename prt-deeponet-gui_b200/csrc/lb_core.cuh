@@ -354,12 +354,14 @@ __device__ __forceinline__ double lb_cell_slots(const Lat<typename M::S>& lat, c
     }
 }
 
-// The same, finding the upstream slots first.
+// The same, finding the upstream slots first (from the slot table when the
+// solve has one: the same slots either way).
 template <class L, class M>
 __device__ __forceinline__ double lb_cell_rw(const Lat<typename M::S>& lat, const FlowMap& fm,
                                              const Grid& g, const LbParams& kc, int k) {
     int src[L::Q];
-    upstream_slots<L>(fm, g, k, src);
+    if (fm.nbr) upstream_slots_table<L>(fm, k, src);
+    else upstream_slots<L>(fm, g, k, src);
     return lb_cell_slots<L, M>(lat, kc, k, src);
 }
 

@@ -273,7 +273,7 @@ static int flow_graph(prt_ctx* ctx) {
     key.aux[0] = F.fluid.p; key.aux[1] = F.partials.p; key.aux[2] = F.ctrl.p;
     key.aux[3] = F.cells.p; key.aux[4] = (void*)F.fm.nbr; key.nf = F.nfluid;
     const char* pdl = std::getenv("PRT_PDL");
-    key.pdl = (pdl && pdl[0] == '1') ? 1 : 0;
+    key.pdl = (pdl && pdl[0] == '0') ? 0 : 1;
     if (!F.graph.exec || !(key == F.key)) {
         CK(build_while_graph(ctx->stream,
                              F.graph, [&](cudaGraphConditionalHandle h, int use) {

@@ -135,15 +135,20 @@ def test_permeability_of_a_slit():
 
 
 def test_programmatic_dependent_launch_gives_the_same_field(monkeypatch):
-    """The optional programmatic-dependent-launch mode of the step kernels
-    (PRT_PDL=1) changes when a kernel starts, never what it computes."""
+    """The step kernels go out with programmatic dependent launch (the
+    default) or plainly (PRT_PDL=0): that changes when a kernel starts,
+    never what it computes.  The cached loop graph is keyed on the switch,
+    so each setting really runs its own launches."""
     from prtlb_gpu import sphere_pack_3d, stokes_d3q19
     g = sphere_pack_3d(24, 0.45, 0)
-    with contextlib.redirect_stdout(io.StringIO()):
-        ref = stokes_d3q19(g, nit=400, tol=0.0, precision="fp32")
-        monkeypatch.setenv("PRT_PDL", "1")
-        got = stokes_d3q19(g, nit=400, tol=0.0, precision="fp32")
-    assert np.array_equal(got, ref)
+    out = {}
+    for mode in ("0", "1", "0"):
+        monkeypatch.setenv("PRT_PDL", mode)
+        with contextlib.redirect_stdout(io.StringIO()):
+            out.setdefault(mode, []).append(
+                stokes_d3q19(g, nit=400, tol=1e-9, precision="fp32"))
+    assert np.array_equal(out["1"][0], out["0"][0])
+    assert np.array_equal(out["0"][1], out["0"][0])
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32", "fp16"])
