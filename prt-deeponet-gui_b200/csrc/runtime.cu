@@ -100,9 +100,6 @@ extern "C" size_t prt_sizeof(int which) {
 // ===========================================================================
 // flow
 // ===========================================================================
-// Transport buffers up to this size outlive prt_adr_end on their context.
-constexpr size_t kAdrKeepBytes = size_t(256) << 20;
-
 // The upstream-slot table: by the working set against the L2 cache
 // (flow_use_nbr), or always / never with PRT_NBR_TABLE=1 / 0.  Both ways
 // give the same slots, so the fields are bit-identical either way.
@@ -855,6 +852,9 @@ extern "C" int prt_adr_means(prt_ctx* ctx, int32_t slot, float* means) {
     CK(cudaStreamSynchronize(ctx->stream));
     return PRT_OK;
 }
+
+// Transport buffers up to this size outlive prt_adr_end on their context.
+constexpr size_t kAdrKeepBytes = size_t(256) << 20;
 
 extern "C" int prt_adr_end(prt_ctx* ctx) {
     if (!ctx) return PRT_E_INVALID;
