@@ -378,6 +378,26 @@ int prt_batch_stats(const prt_batch* b, double* out8);
  * admission control; errors via prt_last_error(NULL). */
 int prt_mem_info(int device, uint64_t* free_bytes, uint64_t* total_bytes);
 
+/* ------------------------------------------------------------------------
+ * Geometry preparation, once per rock before its solves.
+ * ------------------------------------------------------------------------ */
+
+/* The walk from the inlet face through the pore space: for every voxel of
+ * the grid `mat` (nd 2 or 3, dims as in prt_flow_params, C order), the
+ * fewest face-neighbour steps (6 in 3D, 4 in 2D, not periodic) from a voxel
+ * of material pore_code on the face where axis inlet_axis is 0 to it, through
+ * voxels of that material.  steps_out (host, one int32 per voxel) gets the
+ * count for every reached pore voxel, -1 for voxels of another material and
+ * -2 for pore the walk never reaches; *n_reached / *n_pore (either may be
+ * NULL) the reached and all pore voxels.  One walk replaces three reference
+ * routines: keep_inlet_connected (prtlb_3d.py:530-563; its scipy components
+ * touching the face are the reached set), geodesic_steps
+ * (prt_core/conventions.py:72-115) and the relaxed geodesic of the practice
+ * dataset (build_practice_dataset.py:53-73, whose converged value it is). */
+int prt_inlet_walk(prt_ctx* ctx, const uint8_t* mat, int32_t nd, const int32_t* dims,
+                   int32_t pore_code, int32_t inlet_axis, int32_t* steps_out,
+                   int64_t* n_reached, int64_t* n_pore);
+
 /* Host helper, no GPU: the placement loop of the seeded ball packs used as
  * synthetic rocks (prtlb_gpu.geometry.random_pack).  No counterpart in the
  * reference (its build_spheres, build_geometry_3d.py:129-150, makes

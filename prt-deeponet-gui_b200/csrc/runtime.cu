@@ -56,6 +56,7 @@ extern "C" void prt_destroy(prt_ctx* c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     c->adr.release();
+    c->prep.release();
     FlowState& f = c->flow;
     DevBuf* all[] = {&f.f,    &f.fluid, &f.partials, &f.ctrl, &f.out5, &f.count,
                      &f.mat,  &f.vel,   &f.flag,     &f.cnt,  &f.cells, &f.nbr};

@@ -135,6 +135,15 @@ struct AdrState {
     }
 };
 
+// Device buffers of the inlet walk (prep.cu), kept for the next walk.
+struct PrepState {
+    DevBuf mat, steps, flags, counts;
+    void release() {
+        DevBuf* all[] = {&mat, &steps, &flags, &counts};
+        for (DevBuf* b : all) b->release();
+    }
+};
+
 }  // namespace prt
 
 struct prt_ctx {
@@ -146,6 +155,7 @@ struct prt_ctx {
     double timing[4] = {0, 0, 0, 0};
     prt::FlowState flow;
     prt::AdrState adr;
+    prt::PrepState prep;
     bool flow_armed = false;  // flow set up, its time loop not finished
     bool adr_armed = false;   // transport run set up, its time loop not finished
     prt_batch* batch = nullptr;  // the batch holding this context, if any

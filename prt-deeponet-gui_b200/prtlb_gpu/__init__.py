@@ -17,6 +17,7 @@ from .flow import permeability, stokes_d2q9, stokes_d3q19, trt_minus  # noqa: F4
 from .geometry import (assert_finite_distance, coat_with_biofilm,  # noqa: F401
                        keep_inlet_connected, random_pack, sphere_pack_3d, disk_pack_2d)
 from .physics import check_physics  # noqa: F401
+from . import prep  # noqa: F401  (the inlet walk on the GPU: keep_inlet_connected, geodesic_steps, ...)
 
 SOLID, WALL, PORE = 0, 1, 2
 
