@@ -398,6 +398,17 @@ int prt_inlet_walk(prt_ctx* ctx, const uint8_t* mat, int32_t nd, const int32_t* 
                    int32_t pore_code, int32_t inlet_axis, int32_t* steps_out,
                    int64_t* n_reached, int64_t* n_pore);
 
+/* The same walk seeded on the plane where axis `axis` equals `plane`
+ * (0 <= plane < dims[axis]) instead of the face; it runs both ways along the
+ * axis.  A pore component touches planes p and q exactly when the walk from
+ * p reaches plane q: the percolation checks of the dataset builders,
+ * percolates_3d (build_dataset_3d.py:281-286), percolates
+ * (build_dataset_2d.py:290-294), _percolates and keep_percolating_cluster
+ * (build_geometry_3d.py:201-221). */
+int prt_walk_from_plane(prt_ctx* ctx, const uint8_t* mat, int32_t nd, const int32_t* dims,
+                        int32_t pore_code, int32_t axis, int32_t plane, int32_t* steps_out,
+                        int64_t* n_reached, int64_t* n_pore);
+
 /* Host helper, no GPU: the placement loop of the seeded ball packs used as
  * synthetic rocks (prtlb_gpu.geometry.random_pack).  No counterpart in the
  * reference (its build_spheres, build_geometry_3d.py:129-150, makes

@@ -107,10 +107,11 @@ def distance_column(material, convention="ours", inlet_axis=0):
 
 
 def geodesic_relaxed(g, sweeps=None):
-    """The practice-dataset distance (build_practice_dataset.py:53-73):
-    1e9 in pore, 0 on the pore of the x = 0 face, then sweeps of
-    d = min(d, neighbour + 1) over the six face neighbours in turn (no
-    wrap), until a sweep changes nothing or 4 nx sweeps ran; solid 0."""
+    """The practice-dataset distance (build_practice_dataset.py:53-73; in 2D
+    geodesic_2d, build_dataset_2d.py:297-319): 1e9 in pore, 0 on the pore of
+    the x = 0 face, then sweeps of d = min(d, neighbour + 1) over the face
+    neighbours in turn (no wrap), until a sweep changes nothing or 4 nx
+    sweeps ran; solid 0."""
     g = np.asarray(g)
     pore = g == PORE
     big = np.float32(1e9)
@@ -118,13 +119,52 @@ def geodesic_relaxed(g, sweeps=None):
     d[0][pore[0]] = 0.0
     for _ in range(4 * g.shape[0] if sweeps is None else sweeps):
         before = d.copy()
-        for ax in range(3):
+        for ax in range(g.ndim):
             for s in (1, -1):
                 nb = np.roll(d, s, axis=ax)
-                edge = [slice(None)] * 3
+                edge = [slice(None)] * g.ndim
                 edge[ax] = 0 if s > 0 else -1
                 nb[tuple(edge)] = big
                 d = np.where(pore, np.fmin(d, np.where(np.isnan(nb), big, nb) + 1.0), np.nan)
         if np.nanmax(np.abs(np.where(np.isnan(d - before), 0.0, d - before)), initial=0.0) < 1e-6:
             break
     return np.where(np.isnan(d), np.float32(0), d).astype(np.float32)
+
+
+def percolates(g):
+    """Whether one pore component touches both x faces
+    (build_dataset_3d.py:281-286, build_dataset_2d.py:290-294)."""
+    from scipy import ndimage
+    g = np.asarray(g)
+    lab, _ = ndimage.label(g == PORE)
+    first = set(np.unique(lab[0][g[0] == PORE]).tolist()) - {0}
+    last = set(np.unique(lab[-1][g[-1] == PORE]).tolist()) - {0}
+    return bool(first & last)
+
+
+def percolates_between(pore, x_in, x_out):
+    """Whether one component of `pore` touches both planes x = x_in and
+    x = x_out (build_geometry_3d.py:201-205)."""
+    from scipy import ndimage
+    lab, n = ndimage.label(pore)
+    if n == 0:
+        return False
+    return bool((set(np.unique(lab[x_in]).tolist()) - {0}) &
+                (set(np.unique(lab[x_out]).tolist()) - {0}))
+
+
+def keep_percolating_cluster(solid, x_in, x_out):
+    """Pore outside every component touching both planes becomes solid;
+    returns (solid, n_removed), or (solid unchanged, -1) without pore or
+    without such a component (build_geometry_3d.py:208-221)."""
+    from scipy import ndimage
+    solid = np.asarray(solid, bool)
+    pore = ~solid
+    lab, n = ndimage.label(pore)
+    if n == 0:
+        return solid, -1
+    good = (set(np.unique(lab[x_in]).tolist()) - {0}) & (set(np.unique(lab[x_out]).tolist()) - {0})
+    if not good:
+        return solid, -1
+    keep = np.isin(lab, sorted(good))
+    return ~keep, int((pore & ~keep).sum())

@@ -12,6 +12,11 @@
 // voxel of the inlet face to every pore voxel (the reached set is exactly
 // the union of the components touching the face).
 //
+// The same walk from any plane x_a = p (prt_walk_from_plane) serves the
+// percolation checks of the dataset builders (build_dataset_3d.py:281-286,
+// build_dataset_2d.py:290-294, build_geometry_3d.py:201-221): a component
+// touches planes p and q exactly when the walk from p reaches plane q.
+//
 // Here the walk is level-synchronous and pulls: launch L visits every voxel
 // once; a pore voxel not reached yet takes L + 1 if a face neighbour holds
 // L.  A voxel is written only by its own thread, and during launch L the
@@ -34,7 +39,8 @@ constexpr int kLevelsPerChunk = 32;
 struct WalkGrid {
     Grid g;
     FastDiv dz, dy;
-    int axis;  // storage axis of the inlet face (0 x, 1 y, 2 z)
+    int axis;   // storage axis of the seed plane (0 x, 1 y, 2 z)
+    int plane;  // its coordinate along that axis
 };
 
 __device__ __forceinline__ void coords(unsigned c, const WalkGrid& w, int& x, int& y, int& z) {
@@ -45,7 +51,7 @@ __device__ __forceinline__ void coords(unsigned c, const WalkGrid& w, int& x, in
     x = (int)xx;
 }
 
-// steps = 0 on the pore of the inlet face, unreached on the other pore,
+// steps = 0 on the pore of the seed plane, unreached on the other pore,
 // -1 elsewhere; counts[0] += pore voxels.
 __global__ void __launch_bounds__(kWalkThreads)
     walk_init_kernel(const uint8_t* __restrict__ mat, WalkGrid w, int code, int* __restrict__ steps,
@@ -57,7 +63,7 @@ __global__ void __launch_bounds__(kWalkThreads)
         int x, y, z;
         coords(c, w, x, y, z);
         const int along = w.axis == 0 ? x : (w.axis == 1 ? y : z);
-        steps[c] = pore ? (along == 0 ? 0 : kUnreached) : -1;
+        steps[c] = pore ? (along == w.plane ? 0 : kUnreached) : -1;
     }
     const int nb = __syncthreads_count(pore);
     if (threadIdx.x == 0 && nb) atomicAdd(counts, (unsigned long long)nb);
@@ -108,15 +114,18 @@ __global__ void __launch_bounds__(kWalkThreads)
 
 using namespace prt;
 
-extern "C" int prt_inlet_walk(prt_ctx* ctx, const uint8_t* mat, int32_t nd, const int32_t* dims,
-                              int32_t pore_code, int32_t inlet_axis, int32_t* steps_out,
-                              int64_t* n_reached, int64_t* n_pore) {
+extern "C" int prt_walk_from_plane(prt_ctx* ctx, const uint8_t* mat, int32_t nd,
+                                   const int32_t* dims, int32_t pore_code, int32_t axis,
+                                   int32_t plane, int32_t* steps_out, int64_t* n_reached,
+                                   int64_t* n_pore) {
     if (!ctx || !mat || !dims || !steps_out) return fail(ctx, PRT_E_INVALID, "null argument");
     if (nd != 2 && nd != 3) return fail(ctx, PRT_E_INVALID, "nd must be 2 or 3");
     for (int i = 0; i < nd; ++i)
         if (dims[i] <= 0) return fail(ctx, PRT_E_INVALID, "grid dimensions must be positive");
-    if (inlet_axis < 0 || inlet_axis >= nd)
-        return fail(ctx, PRT_E_INVALID, "the inlet axis must be one of the grid's axes");
+    if (axis < 0 || axis >= nd)
+        return fail(ctx, PRT_E_INVALID, "the walk's axis must be one of the grid's axes");
+    if (plane < 0 || plane >= dims[axis])
+        return fail(ctx, PRT_E_INVALID, "the seed plane lies outside the grid");
     const Grid g = make_grid(nd, dims);
     // levels stay below the unreached marker: at most one per pore voxel,
     // plus one chunk
@@ -135,7 +144,8 @@ extern "C" int prt_inlet_walk(prt_ctx* ctx, const uint8_t* mat, int32_t nd, cons
     w.g = g;
     w.dz = make_fastdiv((unsigned)g.nz);
     w.dy = make_fastdiv((unsigned)g.ny);
-    w.axis = nd == 3 ? inlet_axis : (inlet_axis == 0 ? 0 : 2);  // 2D (nx, ny) is (nx, 1, ny)
+    w.axis = nd == 3 ? axis : (axis == 0 ? 0 : 2);  // 2D (nx, ny) is (nx, 1, ny)
+    w.plane = plane;
     const unsigned nb = (unsigned)((g.n + kWalkThreads - 1) / kWalkThreads);
     int* steps = P.steps.as<int>();
     int* flags = P.flags.as<int>();
@@ -166,4 +176,11 @@ extern "C" int prt_inlet_walk(prt_ctx* ctx, const uint8_t* mat, int32_t nd, cons
     if (n_pore) *n_pore = (int64_t)hc[0];
     if (n_reached) *n_reached = (int64_t)hc[1];
     return PRT_OK;
+}
+
+extern "C" int prt_inlet_walk(prt_ctx* ctx, const uint8_t* mat, int32_t nd, const int32_t* dims,
+                              int32_t pore_code, int32_t inlet_axis, int32_t* steps_out,
+                              int64_t* n_reached, int64_t* n_pore) {
+    return prt_walk_from_plane(ctx, mat, nd, dims, pore_code, inlet_axis, 0, steps_out, n_reached,
+                               n_pore);
 }

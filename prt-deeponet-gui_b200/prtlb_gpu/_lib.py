@@ -117,6 +117,11 @@ _PROTOS = {
     "prt_adr_means": (ctypes.c_int, [ctypes.c_void_p, c_i32, ctypes.POINTER(c_f32)]),
     "prt_adr_end": (ctypes.c_int, [ctypes.c_void_p]),
     "prt_adr_release": (ctypes.c_int, [ctypes.c_void_p]),
+    "prt_walk_from_plane": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                           ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
+                                           ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                           ctypes.POINTER(ctypes.c_int64),
+                                           ctypes.POINTER(ctypes.c_int64)]),
     "prt_inlet_walk": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                       ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
                                       ctypes.c_int32, ctypes.c_void_p,

@@ -9,8 +9,13 @@ arguments and outputs:
   geodesic_steps         prt_core/conventions.py:72-115 (the step counts)
   distance_column        prt_core/conventions.py:119-158 (the three scalings
                          of the trunk's distance column, on those counts)
-  geodesic               build_practice_dataset.py:53-73 (the value its
-                         relaxation sweeps converge to)
+  geodesic, geodesic_2d  build_practice_dataset.py:53-73, build_dataset_2d.py:
+                         297-319 (the value their relaxation sweeps converge to)
+  percolates             build_dataset_3d.py:281-286 (percolates_3d),
+                         build_dataset_2d.py:290-294
+  percolates_between,    build_geometry_3d.py:201-221 (_percolates and
+  keep_percolating_cluster  keep_percolating_cluster: two walks, one from each
+                         plane; a component touches both when both reach it)
 
 The reference labels components with scipy and walks with a Python queue,
 one voxel at a time; here each level of the walk is one kernel launch over
@@ -31,11 +36,21 @@ def inlet_walk(mat, pore_code=PORE, inlet_axis=0, *, device=None, ctx=None):
     the count for reached pore voxels (material pore_code), -1 for other
     materials, -2 for pore the walk never reaches.  Returns
     (steps, n_reached, n_pore)."""
+    return walk_from_plane(mat, pore_code, inlet_axis, 0, device=device, ctx=ctx)
+
+
+def walk_from_plane(mat, pore_code=PORE, axis=0, plane=0, *, device=None, ctx=None):
+    """inlet_walk seeded on the plane where `axis` equals `plane` (negative
+    planes count from the far face, as numpy indices do)."""
     mat = np.asarray(mat)
     if mat.ndim not in (2, 3):
         raise ValueError("grid must be 2D or 3D, got %dD" % mat.ndim)
-    if not 0 <= int(inlet_axis) < mat.ndim:
-        raise ValueError("inlet_axis %r is not an axis of a %dD grid" % (inlet_axis, mat.ndim))
+    if not 0 <= int(axis) < mat.ndim:
+        raise ValueError("axis %r is not an axis of a %dD grid" % (axis, mat.ndim))
+    n = mat.shape[int(axis)]
+    if not -n <= int(plane) < n:
+        raise IndexError("plane %r is outside an axis of %d voxels" % (plane, n))
+    plane = int(plane) % n
     if mat.dtype != np.uint8:
         hit = mat == pore_code
         mat8 = hit.astype(np.uint8)
@@ -48,10 +63,10 @@ def inlet_walk(mat, pore_code=PORE, inlet_axis=0, *, device=None, ctx=None):
     steps = np.empty(mat.shape, np.int32)
     nr, npore = ctypes.c_int64(), ctypes.c_int64()
     with ctx.lock:
-        ctx.check(_lib.lib().prt_inlet_walk(ctx.handle, mat8.ctypes.data_as(ctypes.c_void_p),
-                                            mat.ndim, dims, code, int(inlet_axis),
-                                            steps.ctypes.data_as(ctypes.c_void_p),
-                                            ctypes.byref(nr), ctypes.byref(npore)))
+        ctx.check(_lib.lib().prt_walk_from_plane(
+            ctx.handle, mat8.ctypes.data_as(ctypes.c_void_p), mat.ndim, dims, code, int(axis),
+            plane, steps.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nr),
+            ctypes.byref(npore)))
     return steps, int(nr.value), int(npore.value)
 
 
@@ -162,8 +177,55 @@ def geodesic(g, *, device=None, ctx=None):
     g = np.asarray(g)
     if g.ndim != 3:
         raise ValueError("geodesic takes a 3D grid, got %dD" % g.ndim)
+    return _relaxed(g, device, ctx)
+
+
+def geodesic_2d(g, *, device=None, ctx=None):
+    """geodesic on a 2D grid (build_dataset_2d.py:297-319)."""
+    g = np.asarray(g)
+    if g.ndim != 2:
+        raise ValueError("geodesic_2d takes a 2D grid, got %dD" % g.ndim)
+    return _relaxed(g, device, ctx)
+
+
+def _relaxed(g, device, ctx):
     steps, _, _ = inlet_walk(g, PORE, 0, device=device, ctx=ctx)
     d = np.zeros(g.shape, np.float32)
     d[steps >= 0] = steps[steps >= 0].astype(np.float32)
     d[steps == -2] = np.float32(1e9)
     return d
+
+
+def percolates(g, *, device=None, ctx=None):
+    """Whether one pore component touches both x faces, i.e. the walk from
+    the x = 0 face reaches the last x plane (percolates_3d,
+    build_dataset_3d.py:281-286; the 2D builder's percolates,
+    build_dataset_2d.py:290-294)."""
+    g = np.asarray(g)
+    steps, n_reached, _ = inlet_walk(g, PORE, 0, device=device, ctx=ctx)
+    return bool(n_reached) and bool((steps[-1] >= 0).any())
+
+
+def percolates_between(pore, x_in, x_out, *, device=None, ctx=None):
+    """Whether one component of the boolean `pore` touches both planes
+    x = x_in and x = x_out (build_geometry_3d.py:201-205, `_percolates`)."""
+    pore = np.asarray(pore, bool)
+    steps, n_reached, _ = walk_from_plane(pore.view(np.uint8), 1, 0, x_in, device=device, ctx=ctx)
+    return bool(n_reached) and bool((steps[x_out] >= 0).any())
+
+
+def keep_percolating_cluster(solid, x_in, x_out, *, device=None, ctx=None):
+    """Pore outside every component that touches both planes x = x_in and
+    x = x_out becomes solid: returns (solid, n_removed), or the input and -1
+    when there is no pore or no such component (build_geometry_3d.py:208-221).
+    A voxel is kept when the walks from both planes reach it."""
+    solid = np.asarray(solid, bool)
+    pore = (~solid).view(np.uint8)
+    s_in, r_in, n_pore = walk_from_plane(pore, 1, 0, x_in, device=device, ctx=ctx)
+    if n_pore == 0 or r_in == 0:
+        return solid, -1
+    s_out, _, _ = walk_from_plane(pore, 1, 0, x_out, device=device, ctx=ctx)
+    keep = (s_in >= 0) & (s_out >= 0)
+    if not keep.any():
+        return solid, -1
+    return ~keep, int(n_pore - np.count_nonzero(keep))

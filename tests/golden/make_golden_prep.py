@@ -12,6 +12,11 @@ and outputs as compressed .npz files next to this script:
   distance_column        prt_core/conventions.py:119-158 (the three scalings)
   geodesic               3D/tools/build_practice_dataset.py:53-73 (repeated
                          relaxation, 1e9 in unreached pore, 0 in the solid)
+  geodesic_2d            3D/tools/build_dataset_2d.py:297-319 (the same in 2D)
+  percolates_3d          3D/tools/build_dataset_3d.py:281-286 (a pore component
+  percolates (2D)        3D/tools/build_dataset_2d.py:290-294  touches both x faces)
+  _percolates,           3D/tools/build_geometry_3d.py:201-221 (components
+  keep_percolating_cluster                            touching two x planes)
 
 Needs the reference checkout, so it runs in the development container only;
 the fixtures are committed and are all the tests read.
@@ -36,7 +41,11 @@ def load_reference(ref):
     import prtlb_3d
     from prt_core import conventions
     import build_practice_dataset
-    return prtlb_3d, conventions, build_practice_dataset
+    import build_dataset_2d
+    import build_dataset_3d
+    import build_geometry_3d
+    return prtlb_3d, conventions, build_practice_dataset, build_dataset_2d, build_dataset_3d, \
+        build_geometry_3d
 
 
 def grids():
@@ -62,6 +71,9 @@ def grids():
     g[:, 2, 2] = 2
     g[7, 2, 2] = 0  # the column is cut: the far part is unreachable
     out["prep_column3d"] = g
+    g = site((30, 40), 0.66)
+    g[:, 0] = g[:, -1] = 1  # transverse walls, as the 2D builder makes them
+    out["prep_site2d_walls"] = g
     return out
 
 
@@ -75,7 +87,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     args = ap.parse_args()
-    p3, conv, bpd = load_reference(args.ref)
+    p3, conv, bpd, bd2, bd3, bg3 = load_reference(args.ref)
     for name, g in grids().items():
         kept, n_removed = p3.keep_inlet_connected(g.copy())
         arrays = {"mat": g, "kept": np.asarray(kept, np.uint8), "n_removed": np.asarray(n_removed)}
@@ -88,6 +100,17 @@ def main():
             arrays["column_" + c] = np.asarray(conv.distance_column(g, c, 0), np.float32)
         if g.ndim == 3:
             arrays["geodesic"] = np.asarray(bpd.geodesic(np.asarray(kept)), np.float32)
+            arrays["percolates"] = np.asarray(bd3.percolates_3d(g))
+            solid = g != p3.PORE
+            nx = g.shape[0]
+            for k, (xi, xo) in enumerate(((0, nx - 1), (2, nx - 3), (nx // 2, nx // 2))):
+                arrays["perc_between_%d" % k] = np.asarray(bg3._percolates(~solid, xi, xo))
+                kept_s, removed = bg3.keep_percolating_cluster(solid.copy(), xi, xo)
+                arrays["keep_perc_%d" % k] = np.asarray(kept_s, bool)
+                arrays["keep_perc_removed_%d" % k] = np.asarray(removed)
+        else:
+            arrays["geodesic_2d"] = np.asarray(bd2.geodesic_2d(np.asarray(kept)), np.float32)
+            arrays["percolates"] = np.asarray(bd2.percolates(g))
         save(name, **arrays)
 
 

@@ -42,6 +42,21 @@ def test_oracle_matches_reference(name):
             assert _same(O.distance_column(g, c, 0), z["column_" + c]), c
     if "geodesic" in z:
         assert _same(O.geodesic_relaxed(kept), z["geodesic"])
+    if "geodesic_2d" in z:
+        assert _same(O.geodesic_relaxed(kept), z["geodesic_2d"])
+    assert O.percolates(g) == bool(z["percolates"])
+    for k, (xi, xo) in enumerate(_planes(g)):
+        assert O.percolates_between(g == 2, xi, xo) == bool(z["perc_between_%d" % k])
+        ks, r = O.keep_percolating_cluster(g != 2, xi, xo)
+        assert np.array_equal(ks, z["keep_perc_%d" % k]) and r == int(z["keep_perc_removed_%d" % k])
+
+
+def _planes(g):
+    """The plane pairs the golden runs use (3D grids only)."""
+    if g.ndim != 3:
+        return []
+    nx = g.shape[0]
+    return [(0, nx - 1), (2, nx - 3), (nx // 2, nx // 2)]
 
 
 @pytest.mark.gpu
@@ -59,6 +74,13 @@ def test_gpu_walk_matches_reference(name):
         assert _same(prep.distance_column(g, c, 0), z["column_" + c]), c
     if "geodesic" in z:
         assert _same(prep.geodesic(kept), z["geodesic"])
+    if "geodesic_2d" in z:
+        assert _same(prep.geodesic_2d(kept), z["geodesic_2d"])
+    assert prep.percolates(g) == bool(z["percolates"])
+    for k, (xi, xo) in enumerate(_planes(g)):
+        assert prep.percolates_between(g == 2, xi, xo) == bool(z["perc_between_%d" % k])
+        ks, r = prep.keep_percolating_cluster(g != 2, xi, xo)
+        assert np.array_equal(ks, z["keep_perc_%d" % k]) and r == int(z["keep_perc_removed_%d" % k])
 
 
 def _site(shape, p, seed):
@@ -110,6 +132,13 @@ def test_gpu_walk_matches_oracle(case):
     kept, n = prep.keep_inlet_connected(g)
     kept_o, n_o = O.keep_inlet_connected(g)
     assert np.array_equal(kept, kept_o) and n == n_o
+    assert prep.percolates(g) == O.percolates(g)
+    nx = g.shape[0]
+    for xi, xo in ((0, nx - 1), (1, -2), (nx // 3, 2 * nx // 3), (nx - 1, 0)):
+        assert prep.percolates_between(pore, xi, xo) == O.percolates_between(pore, xi, xo)
+        ks, r = prep.keep_percolating_cluster(~pore, xi, xo)
+        ks_o, r_o = O.keep_percolating_cluster(~pore, xi, xo)
+        assert np.array_equal(ks, ks_o) and r == r_o
     if case == "serpentine2d":
         assert np.nanmax(ref) > 900  # about 30 chunks of levels
 
