@@ -81,7 +81,7 @@ int prt_last_timing(const prt_ctx* ctx, double* out4);
 /* sizeof of the ABI structs, for binding checks (needs no GPU):
  * 0 prt_flow_params, 1 prt_flow_info, 2 prt_adr_params,
  * 3 prt_adr_run_params, 4 prt_adr_result, 5 prt_adr_geom,
- * 6 prt_adr_stats; anything else: 0. */
+ * 6 prt_adr_stats, 7 prt_physics_stats; anything else: 0. */
 size_t prt_sizeof(int which);
 
 /* ------------------------------------------------------------------------ */
@@ -408,6 +408,48 @@ int prt_inlet_walk(prt_ctx* ctx, const uint8_t* mat, int32_t nd, const int32_t* 
 int prt_walk_from_plane(prt_ctx* ctx, const uint8_t* mat, int32_t nd, const int32_t* dims,
                         int32_t pore_code, int32_t axis, int32_t plane, int32_t* steps_out,
                         int64_t* n_reached, int64_t* n_pore);
+
+/* ------------------------------------------------------------------------
+ * check_physics (prtlb_3d.py:1632-1843) on the device: the statistics its
+ * rules read, reduced from snapshots out (n_t, ns, voxels) float32 on the
+ * device, with the material grid (pore where mat == pore_code).  The rules
+ * and messages are the host's (prtlb_gpu.physics.check_physics(...,
+ * on_gpu=True)); results that stay on the device are judged without a copy.
+ * ------------------------------------------------------------------------ */
+#define PRT_PHYS_MAX_SNAPSHOTS 256
+
+typedef struct prt_physics_stats {
+    int64_t n_nan, n_inf;        /* over the whole result */
+    int64_t n_triples, n_flips;  /* last donor snapshot: pore triples along x and
+                                    those whose neighbour differences change sign */
+    int32_t has_pore[PRT_MAX_SPECIES];   /* any non-NaN pore value seen */
+    float pore_max[PRT_MAX_SPECIES];     /* over the pore of every snapshot */
+    float pore_min[PRT_MAX_SPECIES];
+    float final_absmax[PRT_MAX_SPECIES]; /* max |value| over the pore of the last one */
+    float mid_max[PRT_PHYS_MAX_SNAPSHOTS];  /* donor, plane x = nx / 2, per snapshot */
+    float end_max[PRT_PHYS_MAX_SNAPSHOTS];  /* donor, plane x = nx - 1 */
+} prt_physics_stats;
+
+/* Copies a host result out (n_t, ns, voxels) and its material grid into the
+ * context; the three calls below then take d_out = NULL / d_mat = NULL for
+ * them (until the next stage or inlet walk on the context). */
+int prt_physics_stage(prt_ctx* ctx, const float* out, const uint8_t* mat, int32_t nd,
+                      const int32_t* dims, int32_t n_t, int32_t ns);
+
+int prt_physics_stats_dev(prt_ctx* ctx, const float* d_out, const uint8_t* d_mat, int32_t nd,
+                          const int32_t* dims, int32_t n_t, int32_t ns, int32_t pore_code,
+                          prt_physics_stats* stats);
+
+/* Donor against chemical j (1 <= j < ns) over the pore of every snapshot:
+ * moments6 = {count, mean0, mean_j, var0, var_j, cov} (population, float64). */
+int prt_physics_moments_dev(prt_ctx* ctx, const float* d_out, const uint8_t* d_mat, int32_t nd,
+                            const int32_t* dims, int32_t n_t, int32_t ns, int32_t pore_code,
+                            int32_t j, double* moments6);
+
+/* max |a_j - scale a_0| over the same voxels, in float32 as numpy forms it. */
+int prt_physics_maxdev_dev(prt_ctx* ctx, const float* d_out, const uint8_t* d_mat, int32_t nd,
+                           const int32_t* dims, int32_t n_t, int32_t ns, int32_t pore_code,
+                           int32_t j, float scale, float* maxdev);
 
 /* Host helper, no GPU: the placement loop of the seeded ball packs used as
  * synthetic rocks (prtlb_gpu.geometry.random_pack).  No counterpart in the

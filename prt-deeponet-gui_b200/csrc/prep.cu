@@ -139,6 +139,7 @@ extern "C" int prt_walk_from_plane(prt_ctx* ctx, const uint8_t* mat, int32_t nd,
     CK(P.flags.ensure(kLevelsPerChunk * sizeof(int)));
     CK(P.counts.ensure(2 * sizeof(unsigned long long)));
     CK(cudaMemcpyAsync(P.mat.p, mat, (size_t)g.n, cudaMemcpyHostToDevice, s));
+    P.staged_mat = -1;  // the buffer now holds the walk's grid
     CK(cudaMemsetAsync(P.counts.p, 0, 2 * sizeof(unsigned long long), s));
     WalkGrid w;
     w.g = g;

@@ -94,6 +94,7 @@ extern "C" size_t prt_sizeof(int which) {
         case 4: return sizeof(prt_adr_result);
         case 5: return sizeof(prt_adr_geom);
         case 6: return sizeof(prt_adr_stats);
+        case 7: return sizeof(prt_physics_stats);
         default: return 0;
     }
 }

@@ -135,11 +135,15 @@ struct AdrState {
     }
 };
 
-// Device buffers of the inlet walk (prep.cu), kept for the next walk.
+// Device buffers of the inlet walk (prep.cu) and of the check_physics
+// reductions (physics.cu), kept for the next call.
 struct PrepState {
-    DevBuf mat, steps, flags, counts;
+    DevBuf mat, steps, flags, counts, keys, sums, out;
+    long long staged_out = -1;  // floats of the staged check_physics result (-1: none)
+    long long staged_mat = -1;  // voxels of the staged material grid
     void release() {
-        DevBuf* all[] = {&mat, &steps, &flags, &counts};
+        DevBuf* all[] = {&mat, &steps, &flags, &counts, &keys, &sums, &out};
+        staged_out = staged_mat = -1;
         for (DevBuf* b : all) b->release();
     }
 };

@@ -117,6 +117,22 @@ _PROTOS = {
     "prt_adr_means": (ctypes.c_int, [ctypes.c_void_p, c_i32, ctypes.POINTER(c_f32)]),
     "prt_adr_end": (ctypes.c_int, [ctypes.c_void_p]),
     "prt_adr_release": (ctypes.c_int, [ctypes.c_void_p]),
+    "prt_physics_stage": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                         ctypes.c_int32, ctypes.c_int32]),
+    "prt_physics_stats_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_void_p]),
+    "prt_physics_moments_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                               ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                               ctypes.c_int32, ctypes.POINTER(c_f64)]),
+    "prt_physics_maxdev_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                              ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_int32, ctypes.c_float,
+                                              ctypes.POINTER(ctypes.c_float)]),
     "prt_walk_from_plane": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                            ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
@@ -159,7 +175,17 @@ _PROTOS = {
                                ctypes.c_void_p, c_i64, ctypes.POINTER(c_i64)]),
 }
 
-SIZEOF_ORDER = [FlowParams, FlowInfo, AdrParams, AdrRunParams, AdrResult, AdrGeom, AdrStats]
+class PhysicsStats(ctypes.Structure):
+    """prt_physics_stats of include/prtlb.h."""
+    _fields_ = [("n_nan", ctypes.c_int64), ("n_inf", ctypes.c_int64),
+                ("n_triples", ctypes.c_int64), ("n_flips", ctypes.c_int64),
+                ("has_pore", ctypes.c_int32 * 8), ("pore_max", ctypes.c_float * 8),
+                ("pore_min", ctypes.c_float * 8), ("final_absmax", ctypes.c_float * 8),
+                ("mid_max", ctypes.c_float * 256), ("end_max", ctypes.c_float * 256)]
+
+
+SIZEOF_ORDER = [FlowParams, FlowInfo, AdrParams, AdrRunParams, AdrResult, AdrGeom, AdrStats,
+                PhysicsStats]
 
 _lib = None
 _lib_lock = threading.Lock()
