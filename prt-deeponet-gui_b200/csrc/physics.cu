@@ -40,10 +40,16 @@ struct PhysGrid {
 // keys: [0, ns) max, [ns, 2 ns) min (as ~key, so atomicMax finds it),
 // [2 ns, 3 ns) final |max|, [3 ns, 3 ns + nt) mid-plane max,
 // [3 ns + nt, 3 ns + 2 nt) outlet-plane max; cnt: nan, inf.
+// Each block gathers its extremes in shared memory and adds them to the
+// global keys once, so the global atomics are one per key per block.
 __global__ void __launch_bounds__(kPhysThreads)
     phys_extremes_kernel(const float* __restrict__ out, const uint8_t* __restrict__ mat, int pore,
                          PhysGrid p, unsigned* __restrict__ keys,
                          unsigned long long* __restrict__ cnt) {
+    __shared__ unsigned sk[3 * PRT_MAX_SPECIES + 2 * PRT_PHYS_MAX_SNAPSHOTS];
+    const int nkeys = 3 * p.ns + 2 * p.nt;
+    for (int i = threadIdx.x; i < nkeys; i += kPhysThreads) sk[i] = 0;
+    __syncthreads();
     const long long total = (long long)p.nt * p.ns * p.n;
     unsigned long long nnan = 0, ninf = 0;
     for (long long e = (long long)blockIdx.x * kPhysThreads + threadIdx.x; e < total;
@@ -59,18 +65,21 @@ __global__ void __launch_bounds__(kPhysThreads)
         }
         if (isinf(v)) ++ninf;
         if (mat[c] == pore) {
-            atomicMax(keys + j, fkey(v));
-            atomicMax(keys + p.ns + j, ~fkey(v));
-            if (t == p.nt - 1) atomicMax(keys + 2 * p.ns + j, fkey(fabsf(v)));
+            atomicMax(sk + j, fkey(v));
+            atomicMax(sk + p.ns + j, ~fkey(v));
+            if (t == p.nt - 1) atomicMax(sk + 2 * p.ns + j, fkey(fabsf(v)));
         }
         if (j == 0) {
             const int x = (int)fast_div((unsigned)c, p.dyz);
-            if (x == p.nx / 2) atomicMax(keys + 3 * p.ns + t, fkey(v));
-            if (x == p.nx - 1) atomicMax(keys + 3 * p.ns + p.nt + t, fkey(v));
+            if (x == p.nx / 2) atomicMax(sk + 3 * p.ns + t, fkey(v));
+            if (x == p.nx - 1) atomicMax(sk + 3 * p.ns + p.nt + t, fkey(v));
         }
     }
     if (nnan) atomicAdd(cnt, nnan);
     if (ninf) atomicAdd(cnt + 1, ninf);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nkeys; i += kPhysThreads)
+        if (sk[i]) atomicMax(keys + i, sk[i]);
 }
 
 // Pore triples along x of the last donor snapshot and the ones whose two
