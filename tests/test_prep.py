@@ -167,3 +167,27 @@ def test_gpu_walk_edges_and_refusals():
                                    0, out.ctypes.data_as(ctypes.c_void_p), None, None)
     assert rc == _lib.PRT_E_INVALID
     assert PrtError  # the module's error type is what ctx.check raises
+
+
+def test_argument_checks_need_no_gpu():
+    """The wrappers refuse bad shapes, axes, planes and conventions before
+    any device call, with the reference's error types."""
+    from prtlb_gpu import prep
+    g = np.zeros((4, 3, 2), np.uint8)
+    with pytest.raises(ValueError):
+        prep.inlet_walk(np.zeros((2, 2, 2, 2), np.uint8))
+    with pytest.raises(ValueError):
+        prep.inlet_walk(g, inlet_axis=3)
+    with pytest.raises(IndexError):
+        prep.walk_from_plane(g, 2, 0, 4)
+    with pytest.raises(ValueError):
+        prep.distance_column(g, "reversed")
+    with pytest.raises(ValueError):
+        prep.geodesic(np.zeros((4, 4), np.uint8))
+    with pytest.raises(ValueError):
+        prep.geodesic_2d(g)
+    assert prep.pore_mask(np.array([[0, 1]], np.uint8)).tolist() == [[False, True]]
+    assert prep.pore_mask(np.array([[0, 2, 1]], np.uint8)).tolist() == [[False, True, False]]
+    s = prep._seeded(0.1, 3)
+    assert s.dtype == np.float32 and s[3] == ((np.float32(0.1) + np.float32(1)) + np.float32(1)) + \
+        np.float32(1)
