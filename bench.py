@@ -628,7 +628,11 @@ def main():
                            "flow_iters": r["iters"], "transport_steps": r["adr_steps"],
                            "voxels": r["ncell"], "pore_voxels": r["nfluid"],
                            "e2e_ms": r["e2e_ms"], "e2e_split": r["e2e_split"],
-                           "solves_per_hour": 3.6e6 / r["ms_per_step"] * world}}
+                           "solves_per_hour": 3.6e6 / r["ms_per_step"] * world,
+                           # each loop on its own, over all voxels (one chemical)
+                           "flow_glups": r["iters"] * r["ncell"] / max(r["flow_ms"] * 1e6, 1e-9),
+                           "transport_gcell_species_per_s":
+                               r["adr_steps"] * r["ncell"] / max(r["adr_ms"] * 1e6, 1e-9)}}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()
