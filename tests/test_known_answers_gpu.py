@@ -134,6 +134,85 @@ def abiotic_conversion(oracle=False):
     return g, res
 
 
+def _sound_run(oracle=False):
+    """The four-chemical run of 16f (prtlb_3d.py:2368-2373): a walled channel,
+    the default chemistry, Pe 30, Da 1, to the stop rule."""
+    from prtlb_gpu.chemistry import default_chemistry
+    g = np.full((40, 8), PORE, np.uint8)
+    g[:, 0] = g[:, -1] = SOLID
+    v = np.zeros((3, 40, 8), np.float32)
+    v[0] = 1.0
+    ch = default_chemistry(4)
+    info = {}
+    with contextlib.redirect_stdout(io.StringIO()):
+        o, _ = _adr(oracle)(g, v, pe=30.0, da=1.0, n_t=4, n_species=4, chem=ch, info=info)
+    return g, v, ch, o, info
+
+
+def planted_complaints(on_gpu=False, oracle=False):
+    """16f (:2368-2397): check_physics is quiet on a sound run and names each
+    planted fault: product above its bound, a negative chemical, a vanished
+    one, runaway biomass, a checkerboard along the flow (but not across it)."""
+    from prtlb_gpu.physics import check_physics
+    g, _, ch, o, _ = _sound_run(oracle)
+    cp = lambda x: check_physics(x, g, chem=ch, on_gpu=on_gpu)  # noqa: E731
+    got = {"sound": cp(o)}
+    b = o.copy(); b[:, 2] = 5.0
+    got["product"] = cp(b)
+    b = o.copy(); b[:, 1] = -0.5 * (g == PORE)
+    got["negative"] = cp(b)
+    b = o.copy(); b[:, 0] = 0.0
+    got["zero"] = cp(b)
+    b = o.copy(); b[:, 3] = 500.0
+    got["runaway"] = cp(b)
+    xs = np.arange(40)[:, None] * np.ones((1, 8))
+    b = o.copy(); b[-1, 0] = np.where(g == PORE, 0.5 + 0.4 * ((-1.0) ** xs), 0.0)
+    got["along"] = cp(b)
+    zs = np.arange(8)[None, :] * np.ones((40, 1))
+    b = o.copy(); b[-1, 0] = np.where(g == PORE, 0.5 + 0.4 * ((-1.0) ** zs), 0.0)
+    got["across"] = cp(b)
+    return got
+
+
+def _check_planted(got):
+    assert got["sound"] == []
+    assert any("P reaches" in c for c in got["product"])
+    assert any("negative" in c for c in got["negative"])
+    assert any("exactly zero" in c for c in got["zero"])
+    assert any("runaway" in c for c in got["runaway"])
+    assert any("checkerboard" in c for c in got["along"])
+    assert not any("checkerboard" in c for c in got["across"])
+
+
+def stop_point_gap(oracle=False):
+    """16g (:2399-2421): when the stop rule fires, the slowest chemicals
+    (product, biomass) are within 1 % of a run 16 times longer."""
+    g, v, ch, stopped, info = _sound_run(oracle)
+    with contextlib.redirect_stdout(io.StringIO()):
+        long_run, _ = _adr(oracle)(g, v, pe=30.0, da=1.0, n_t=4, n_species=4, chem=ch,
+                                   steps=info["steps"] * 16)
+    p = g == PORE
+    return [abs(float(stopped[-1, j][p].mean()) - float(long_run[-1, j][p].mean())) /
+            max(abs(float(long_run[-1, j][p].mean())), 1e-9) for j in (2, 3)]
+
+
+def axial_peclet_fronts(oracle=False):
+    """16h (:2423-2434): the Peclet number is taken against the axial
+    velocity, so a transverse component does not move the front."""
+    g = np.full((40, 16), PORE, np.uint8)
+    v_ax = np.zeros((3, 40, 16), np.float32)
+    v_ax[0] = 1.0
+    v_tt = v_ax.copy()
+    v_tt[1] = 0.6
+    fronts = []
+    for v in (v_ax, v_tt):
+        with contextlib.redirect_stdout(io.StringIO()):
+            o, _ = _adr(oracle)(g, v, pe=30.0, da=0.0, n_t=2, n_species=1, steps=200,
+                                chem=_tracer())
+        fronts.append(float(np.argmax(o[-1, 0].mean(1) < 0.5)))
+    return fronts
+
+
 def grid_peclet_warnings():
     from prtlb_gpu import solve_adr
     g, v = _channel(80, 8)
@@ -191,6 +270,23 @@ def test_abiotic_donor_becomes_product():
         assert abs(ac + p - 1.0) < 0.01, (ac, p)
         assert not check_physics(o, g, chem=ch, da_abio=da_a)
         prev = p
+
+
+@gpu
+@pytest.mark.parametrize("on_gpu", [False, True])
+def test_check_physics_names_each_planted_fault(on_gpu):
+    _check_planted(planted_complaints(on_gpu=on_gpu))
+
+
+@gpu
+def test_stop_point_is_within_one_percent_of_settled():
+    assert max(stop_point_gap()) < 0.01
+
+
+@gpu
+def test_peclet_is_taken_against_the_axial_velocity():
+    a, b = axial_peclet_fronts()
+    assert abs(a - b) <= 1
 
 
 def _poiseuille_peak(nd, H):
