@@ -63,10 +63,9 @@ SEED = 0
 FORCE, TAU, FLOW_TOL, FLOW_NIT = 2e-6, 0.8, 1e-6, 30000
 ADR_STEPS = None  # None: run to the reference's stop rule
 # DRAM bytes (read + write) of one lb_step_kernel launch from an ncu capture
-# (cache flushed before the launch), by grid edge: profiles/
-# lb_step_kernel_plain3d_64.md and lb_step_kernel_sphere128.md.  At 64^3
-# they include the upstream-slot table (72 B per pore voxel, 8.4 MB), which
-# the solve reads instead of the voxel map because its working set fits in L2.
+# (cache flushed before the launch), by grid edge.  At 64^3 they include the
+# upstream-slot table (72 B per pore voxel, 8.4 MB), which the solve reads
+# instead of the voxel map because its working set fits in L2.
 TRAFFIC_PER_LAUNCH = {64: 25157632, 128: 176652032}
 PE, DA, KS, N_T = 10.0, 1.0, 0.5, 5
 METRIC = "D3Q19 TRT+ADR GLUPS"
@@ -79,6 +78,18 @@ WORKLOAD = ("plain-3d: 64^3 sphere pack (r U[4,7], porosity 0.45, seed 0), D3Q19
 def geometry():
     from prtlb_gpu.geometry import sphere_pack_3d
     return sphere_pack_3d(EDGE, POROSITY, SEED)
+
+
+def host_geometry():
+    """The same pack from the NumPy placement loop of prtlb_gpu/geometry.py,
+    loaded as a plain module by its path: neither the package nor its
+    library enters the process (the CPU arms use this)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "prt_host_geometry", os.path.join(PKG, "prtlb_gpu", "geometry.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.random_pack((EDGE,) * 3, POROSITY, 4.0, 7.0, seed=SEED, native=False)
 
 
 def peaks():
@@ -510,18 +521,17 @@ def cpu_sample(args_tuple):
     """Time a bounded sample of the workload with the NumPy oracle:
     `its` flow iterations and `steps` transport steps on the 64^3 pack."""
     its, steps = args_tuple
-    sys.path[:0] = [ROOT, PKG]
+    sys.path[:0] = [ROOT]
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     from oracle import prtlb_oracle as O
-    from prtlb_gpu.chemistry import monod_chemistry
-    g = geometry()
+    g = host_geometry()
     t0 = time.perf_counter()
     v = O.stokes(g, nit=its, force=FORCE, tau_lb=TAU, tol=0.0)
     t1 = time.perf_counter()
     v[0] += 1e-4 * (g == 2)  # a moving field for the transport sample
     with contextlib.redirect_stdout(io.StringIO()):
         O.solve_adr(g, v, pe=PE, da=DA, n_t=2, n_species=1, steps=steps,
-                    chem=monod_chemistry(KS))
+                    chem=O.monod_chemistry(KS))
     t2 = time.perf_counter()
     n = g.size
     return {"flow_s": t1 - t0, "adr_s": t2 - t1, "updates": float(its + steps) * n,

@@ -140,10 +140,12 @@ int prt_flow_dev(prt_ctx* ctx, const uint8_t* d_mat, const prt_flow_params* p,
  * file-scope __device__ array in the library, which every GPU that loads
  * the library holds until exit; a grid that does not fit (64^3 D3Q19 at
  * float32 does) is refused with PRT_E_INVALID and a message giving both
- * sizes.  The first call on a device looks up the array's address; make it
- * before any stream capture.  Calls share the array: calls that overlap on
- * the GPU race and must be serialised.  Runs on the current device; errors
- * are read with prt_last_error(NULL). */
+ * sizes.  Every call looks up the array's address on the current device
+ * (cudaGetSymbolAddress) and runs there; nothing is cached between calls.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised.  The call returns after its work on the stream has finished,
+ * also when it fails after its first launch.  Errors are read with
+ * prt_last_error(NULL), which a successful call leaves empty. */
 int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, float* d_vel_out,
                      prt_flow_info* info, void* stream);
 

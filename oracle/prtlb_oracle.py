@@ -165,6 +165,20 @@ def default_chemistry(n_species=2):
     return c
 
 
+def monod_chemistry(ks=0.5):
+    """Single-substrate Monod as the reference's Chemistry(names=["C"],
+    inlet=[1], c_init=[0], d_rel=[1], immobile=[False], ks_donor=ks) holds it
+    (settings_and_units.py:1834-1929: no decay given, so decay_for is 0), as
+    a plain namespace for the oracle."""
+    c = default_chemistry(1)
+    c.names = ["C"]
+    c.ks_donor = float(ks)
+    c.source = "monod"
+    c.decay_for = lambda nx: 0.0
+    c.truncate = lambda n: c
+    return c
+
+
 def solve_adr(mat, vel, pe, da, n_t, n_species=2, steps=None, tol=2e-3, max_steps=100000,
               info=None, ratio=1.12, chem=None, da_abio=0.0, on_progress=None,
               dtype=np.float32, record_means=None):

@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
         FlowCtrl* ctrl = sj.ctrl;
         const long long it = __ldcg(&ctrl->it_base);
         const bool run = !__ldcg(&ctrl->done) && it < __ldcg(&ctrl->nit);
-        const bool check = __ldcg(&ctrl->tol) > 0 && ((it + 1) % __ldcg(&ctrl->every)) == 0;
+        const bool check = ((it + 1) % __ldcg(&ctrl->every)) == 0;  // the sampled iterations
         if (!run) {  // uniform over the block
             __syncthreads();  // every thread has read ctrl before sj may change
             continue;

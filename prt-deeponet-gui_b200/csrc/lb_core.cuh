@@ -404,12 +404,18 @@ __device__ __forceinline__ double block_sum_fixed(const double* p, int n) {
 }
 
 // FlowConvergence bookkeeping (prtlb_3d.py:220-235) once the iterations up
-// to `end` are done; `check` says whether the mean |u_x| of iteration end-1
-// (sum s over the pore) is sampled at this point.
-__device__ __forceinline__ void flow_ctrl_advance(FlowCtrl* c, long long end, bool check,
+// to `end` are done; `sample` says whether the mean |u_x| of iteration end-1
+// (sum s over the pore) was taken at this point (every `every` iterations).
+// A sampled sum that is not finite stops the solve at once: the reference
+// would run on to its cap (a NaN change never meets the tolerance) and then
+// refuse the field, so stopping early changes only how long a doomed solve
+// takes, never a finite result.
+__device__ __forceinline__ void flow_ctrl_advance(FlowCtrl* c, long long end, bool sample,
                                                   double s) {
     c->iters = end;
-    if (check) {
+    if (sample && !isfinite(s)) {
+        c->nonfinite = 1;
+    } else if (sample && c->tol > 0) {
         const double u = c->nfluid > 0 ? s / (double)c->nfluid : 0.0;
         if (c->has_prev) {
             c->change = fabs(u - c->prev) / fmax(fabs(u), 1e-30);
@@ -419,7 +425,7 @@ __device__ __forceinline__ void flow_ctrl_advance(FlowCtrl* c, long long end, bo
         c->has_prev = 1;
     }
     c->it_base = end;
-    if (c->converged || end >= c->nit) c->done = 1;
+    if (c->converged || c->nonfinite || end >= c->nit) c->done = 1;
 }
 
 }  // namespace prt

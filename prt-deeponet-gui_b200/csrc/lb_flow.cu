@@ -61,14 +61,16 @@ __global__ void flow_check_kernel(FlowCtrl* ctrl, const double* __restrict__ par
     const long long base = ctrl->it_base;
     const long long end = min(base + (long long)ctrl->every, ctrl->nit);
     const bool full = (end - base) == ctrl->every;
+    // the partials of the chunk's last iteration are summed at every full
+    // chunk: for the convergence mean and the non-finite stop
     double s = 0.0;
-    if (!done_before && full && ctrl->tol > 0) s = block_sum_fixed(partials, nb);
+    if (!done_before && full) s = block_sum_fixed(partials, nb);
     if (threadIdx.x != 0) return;
     if (done_before) {
         if (use_handle) cudaGraphSetConditional(h, 0);
         return;
     }
-    flow_ctrl_advance(ctrl, end, ctrl->tol > 0 && full && (end % ctrl->every) == 0, s);
+    flow_ctrl_advance(ctrl, end, full && (end % ctrl->every) == 0, s);
     if (use_handle) cudaGraphSetConditional(h, ctrl->done ? 0 : 1);
 }
 

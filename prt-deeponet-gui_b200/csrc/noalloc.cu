@@ -20,16 +20,19 @@
 //     pore count) itself.  Calls whose work overlaps on the GPU (different
 //     streams or threads at the same time) race on the array and give wrong
 //     results: serialise them.
-//   - The first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before any stream capture.
-//   - The solve runs on the calling thread's current device.
+//   - Every call looks up the array's device address (cudaGetSymbolAddress)
+//     on the calling thread's current device, in the CUDA context current
+//     there, and runs the solve on that device.  Nothing is cached between
+//     calls, so a device reset or another current context between calls is
+//     seen by the next call.
+//   - The call returns only after its work on the stream has finished, on
+//     success and on every error after the first launch, so the caller may
+//     free or reuse d_vel_out as soon as it returns.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "prt_internal.h"
@@ -39,14 +42,10 @@ using namespace prt;
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = 48u << 20;
-constexpr int kMaxDevices = 64;
 
 // The scratch itself.  In host code this name is only a stand-in for the
 // device symbol; the kernels get the address from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_scratch[kNoAllocScratchBytes];
-
-std::mutex g_mu;
-void* g_addr[kMaxDevices] = {nullptr};
 
 // the message goes where prt_last_error(NULL) reads it
 int fail(int code, const std::string& msg) {
@@ -55,19 +54,6 @@ int fail(int code, const std::string& msg) {
 }
 
 size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
-
-// Device address of g_scratch on the current device, looked up once.
-cudaError_t scratch_addr(int dev, void** out) {
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e != cudaSuccess) return e;
-        g_addr[dev] = p;
-    }
-    *out = g_addr[dev];
-    return cudaSuccess;
-}
 
 __global__ void noalloc_ctrl_kernel(FlowCtrl* ctrl, const long long* count, long long nit,
                                     double tol, int every) {
@@ -83,6 +69,8 @@ __global__ void noalloc_ctrl_kernel(FlowCtrl* ctrl, const long long* count, long
     ctrl->done = nit == 0 ? 1 : 0;
     ctrl->has_prev = 0;
     ctrl->converged = 0;
+    ctrl->nonfinite = 0;
+    ctrl->pad = 0;
 }
 
 }  // namespace
@@ -95,20 +83,12 @@ __global__ void noalloc_ctrl_kernel(FlowCtrl* ctrl, const long long* count, long
                         std::string(#expr) + ": " + cudaGetErrorString(_e));           \
     } while (0)
 
-extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, float* d_vel_out,
-                                prt_flow_info* info, void* stream) {
-    if (!p || !d_mat || !d_vel_out) return fail(PRT_E_INVALID, "null argument");
-    if (p->nd != 2 && p->nd != 3) return fail(PRT_E_INVALID, "nd must be 2 or 3");
-    for (int i = 0; i < p->nd; ++i)
-        if (p->dims[i] <= 0) return fail(PRT_E_INVALID, "grid dimensions must be positive");
-    if (!(p->tau > 0.5))
-        return fail(PRT_E_INVALID, "tau must exceed 0.5; the viscosity (tau-1/2)/3 is negative "
-                                   "below it and the solver cannot run.");
-    if (p->every <= 0 || (p->every & 1))
-        return fail(PRT_E_INVALID, "the convergence interval must be a positive even number");
-    if (p->precision < PRT_FP64 || p->precision > PRT_FP32_F32)
-        return fail(PRT_E_INVALID, "unknown precision");
-    if (p->nit < 0) return fail(PRT_E_INVALID, "negative iteration cap");
+namespace {
+
+// The solve after the argument checks; `launched` is set once work may be
+// queued on the stream.
+int noalloc_solve(const uint8_t* d_mat, const prt_flow_params* p, float* d_vel_out,
+                  prt_flow_info* info, cudaStream_t s, bool& launched) {
     Grid g;
     g.nx = p->dims[0];
     g.ny = p->nd == 3 ? p->dims[1] : 1;
@@ -137,11 +117,9 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
                     "this grid needs " + std::to_string(need) + " bytes of scratch but the "
                     "allocation-free solve has " + std::to_string(kNoAllocScratchBytes) +
                     "; use prt_flow / prt_flow_dev");
-    int dev = 0;
-    NCK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(PRT_E_INVALID, "device ordinal too large");
+    // the array's address in the context current on this thread's device
     void* base = nullptr;
-    NCK(scratch_addr(dev, &base));
+    NCK(cudaGetSymbolAddress(&base, g_scratch));
     unsigned char* sb = static_cast<unsigned char*>(base);
     FlowCtrl* ctrl = reinterpret_cast<FlowCtrl*>(sb + o_ctrl);
     long long* count = reinterpret_cast<long long*>(sb + o_count);
@@ -152,51 +130,28 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
     int* cells = reinterpret_cast<int*>(sb + o_cells);
     int* imap = reinterpret_cast<int*>(sb + o_imap);
     void* f = sb + o_lat;
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
 
-    // constants (_trt_minus, prtlb_3d.py:130-139; Guo term prtlb_3d.py:439-440)
-    LbParams k;
-    const double om_p = 1.0 / p->tau;
-    const double om_m = 1.0 / (p->magic / (1.0 / om_p - 0.5) + 0.5);
-    k.omp = om_p;
-    k.omm = om_m;
-    k.half_g = 0.5 * p->force;
-    for (int i = 0; i < 9; ++i) k.guo[i] = 0.0;
-    if (p->nd == 3) {
-        const int pa[9] = {1, 3, 5, 7, 9, 11, 13, 15, 17};
-        const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
-        for (int i = 0; i < 9; ++i) {
-            const double w = pa[i] < 7 ? 1.0 / 18.0 : 1.0 / 36.0;
-            k.guo[i] = w * (1 - 0.5 * om_m) * 3.0 * p->force * ex[pa[i]];
-        }
-    } else {
-        const int pa[4] = {1, 2, 5, 6};
-        const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
-        for (int i = 0; i < 4; ++i) {
-            const double w = pa[i] < 5 ? 1.0 / 9.0 : 1.0 / 36.0;
-            k.guo[i] = w * (1 - 0.5 * om_m) * 3.0 * p->force * ex[pa[i]];
-        }
-    }
     float scale = 1.f;
     if (p->precision == PRT_FP16) {
         const double g0 = std::fabs(p->force) > 0 ? std::fabs(p->force) : 1e-6;
         scale = (float)std::ldexp(1.0, (int)std::floor(std::log2(1.0 / g0)));
     }
-    k.scale = scale;
-    k.inv_scale = 1.0f / scale;
+    LbParams k;
+    fill_lbconst(k, p->nd, p->force, p->tau, p->magic, scale);
 
     // everything that must start at zero is cleared here: the array keeps
     // whatever the previous call left
     // pore-only layout: flags, count, pore list, voxel -> slot map
+    launched = true;
     NCK(flow_launch_flags(d_mat, g.n, 2, flag, s));
     NCK(adr_launch_compact(flag, g.n, cnt, count, nullptr, s));
     long long nfluid = 0;
     NCK(cudaMemcpyAsync(&nfluid, count, sizeof(nfluid), cudaMemcpyDeviceToHost, s));
     NCK(cudaStreamSynchronize(s));
-    NCK(adr_launch_compact(flag, g.n, cnt, count, cells, s));
-    NCK(cudaMemsetAsync(imap, 0xff, (size_t)g.n * 4, s));
     if ((long long)2 * Q * nfluid >= (1ll << 31))
         return fail(PRT_E_INVALID, "more pore voxels than the 32-bit lattice offsets hold");
+    NCK(adr_launch_compact(flag, g.n, cnt, count, cells, s));
+    NCK(cudaMemsetAsync(imap, 0xff, (size_t)g.n * 4, s));
     FlowMap fm;
     fm.ys = coord_bits(g.nz);
     fm.xs = fm.ys + coord_bits(g.ny);
@@ -215,12 +170,12 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
     // the time loop, launched directly (no graph objects), chunk by chunk;
     // kernels after the stop are no-ops, so a few chunks go out per check
     const long long chunks = (p->nit + p->every - 1) / p->every;
-    long long launched = 0;
+    long long sent = 0;
     FlowCtrl hc;
     memset(&hc, 0, sizeof(hc));
     hc.done = p->nit == 0 ? 1 : 0;
-    while (!hc.done && launched < chunks) {
-        for (int r = 0; r < 8 && launched < chunks; ++r, ++launched) {
+    while (!hc.done && sent < chunks) {
+        for (int r = 0; r < 8 && sent < chunks; ++r, ++sent) {
             for (int kk = 0; kk < p->every; ++kk)
                 NCK(flow_launch_step(p->nd, p->precision, (kk & 1) != 0, kk == p->every - 1, f,
                                      fm, g, k, ctrl, kk, parts, s));
@@ -253,4 +208,30 @@ extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, 
         info->fp16_scale = scale;
     }
     return PRT_OK;
+}
+
+}  // namespace
+
+extern "C" int prt_flow_noalloc(const uint8_t* d_mat, const prt_flow_params* p, float* d_vel_out,
+                                prt_flow_info* info, void* stream) {
+    prt::set_noctx_error("");  // a success leaves no earlier message behind
+    if (!p || !d_mat || !d_vel_out) return fail(PRT_E_INVALID, "null argument");
+    if (p->nd != 2 && p->nd != 3) return fail(PRT_E_INVALID, "nd must be 2 or 3");
+    for (int i = 0; i < p->nd; ++i)
+        if (p->dims[i] <= 0) return fail(PRT_E_INVALID, "grid dimensions must be positive");
+    if (!(p->tau > 0.5))
+        return fail(PRT_E_INVALID, "tau must exceed 0.5; the viscosity (tau-1/2)/3 is negative "
+                                   "below it and the solver cannot run.");
+    if (p->every <= 0 || (p->every & 1))
+        return fail(PRT_E_INVALID, "the convergence interval must be a positive even number");
+    if (p->precision < PRT_FP64 || p->precision > PRT_FP32_F32)
+        return fail(PRT_E_INVALID, "unknown precision");
+    if (p->nit < 0) return fail(PRT_E_INVALID, "negative iteration cap");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    bool launched = false;
+    const int rc = noalloc_solve(d_mat, p, d_vel_out, info, s, launched);
+    // a failure after the first launch still waits for what was queued, so
+    // no kernel of this call writes d_vel_out or the array after the return
+    if (rc != PRT_OK && launched) cudaStreamSynchronize(s);
+    return rc;
 }

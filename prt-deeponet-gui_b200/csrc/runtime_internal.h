@@ -169,7 +169,6 @@ struct prt_ctx {
 
 namespace prt {
 
-
 inline int fail(prt_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
@@ -255,38 +254,6 @@ inline Grid make_grid(int nd, const int32_t* dims) {
     }
     g.n = (long long)g.nx * g.ny * g.nz;
     return g;
-}
-
-inline void fill_lbconst(LbParams& k, int nd, double force, double tau, double magic, float scale) {
-    // _trt_minus (prtlb_3d.py:130-139)
-    const double om_p = 1.0 / tau;
-    const double lam_p = 1.0 / om_p - 0.5;
-    const double om_m = 1.0 / (magic / lam_p + 0.5);
-    k.omp = om_p;
-    k.omm = om_m;
-    k.half_g = 0.5 * force;
-    for (int p = 0; p < 9; ++p) k.guo[p] = 0.0;
-    // first member of each pair and its x component
-    if (nd == 3) {
-        // pairs (1,2) (3,4) ... (17,18); e_x of 1,7,9,11,13 is +1, of 3,5,15,17 is 0
-        const int pa[9] = {1, 3, 5, 7, 9, 11, 13, 15, 17};
-        const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
-        for (int p = 0; p < 9; ++p) {
-            const int a = pa[p];
-            const double w = a < 7 ? 1.0 / 18.0 : 1.0 / 36.0;
-            k.guo[p] = w * (1 - 0.5 * om_m) * 3.0 * force * ex[a];
-        }
-    } else {
-        const int pa[4] = {1, 2, 5, 6};
-        const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
-        for (int p = 0; p < 4; ++p) {
-            const int a = pa[p];
-            const double w = a < 5 ? 1.0 / 9.0 : 1.0 / 36.0;
-            k.guo[p] = w * (1 - 0.5 * om_m) * 3.0 * force * ex[a];
-        }
-    }
-    k.scale = scale;
-    k.inv_scale = 1.0f / scale;
 }
 
 

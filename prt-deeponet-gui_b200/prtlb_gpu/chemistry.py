@@ -103,14 +103,15 @@ class Chemistry(object):
                          sorption=self.sorption)
 
     def describe(self):
-        lines = ["  %-6s %9s %9s %8s %9s" % ("name", "feed", "at t=0", "D/D_ref", "moves")]
+        """One line per chemical: its name, feed, start value, diffusivity
+        ratio and whether it is transported."""
+        out = []
         for i, nm in enumerate(self.names):
-            fed = self.inlet[i]
-            lines.append("  %-6s %9s %9.4g %8.3g %9s"
-                         % (nm, "no feed" if fed != fed else "%.4g" % fed,
-                            self.c_init[i], self.d_rel[i],
-                            "no" if self.immobile[i] else "yes"))
-        return "\n".join(lines)
+            feed = "unfed" if self.inlet[i] != self.inlet[i] else "feed=%g" % self.inlet[i]
+            out.append("%s: %s, c0=%g, D/D_ref=%g, %s"
+                       % (nm, feed, self.c_init[i], self.d_rel[i],
+                          "immobile" if self.immobile[i] else "mobile"))
+        return "; ".join(out)
 
 
 def default_chemistry(n_species=2):

@@ -8,7 +8,7 @@ checkout) on small seeded cases and saves inputs and outputs as compressed
 the development container only; the fixtures it writes are committed and are
 all the tests read.
 
-    python tests/golden/make_golden.py [--ref /path/to/reference]
+    python tests/golden/make_golden.py --ref /path/to/reference
 
 Cases (every one small enough for the reference to finish in seconds):
   flow_*   stokes_d2q9 / stokes_d3q19: slits (fixed iteration counts and
@@ -72,7 +72,8 @@ def info_arrays(info, prefix="info_"):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True,
+                    help="path of the reference checkout")
     args = ap.parse_args()
     p2, p3, su = load_reference(args.ref)
     PORE, SOLID = p3.PORE, p3.SOLID

@@ -21,7 +21,7 @@ and outputs as compressed .npz files next to this script:
 Needs the reference checkout, so it runs in the development container only;
 the fixtures are committed and are all the tests read.
 
-    python tests/golden/make_golden_prep.py [--ref /path/to/reference]
+    python tests/golden/make_golden_prep.py --ref /path/to/reference
 """
 
 import argparse
@@ -85,7 +85,8 @@ def save(name, **arrays):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True,
+                    help="path of the reference checkout")
     args = ap.parse_args()
     p3, conv, bpd, bd2, bd3, bg3 = load_reference(args.ref)
     for name, g in grids().items():

@@ -172,3 +172,19 @@ def test_upstream_slot_table_gives_the_same_field(monkeypatch, precision):
     assert np.array_equal(out["0"][0], out["1"][0])
     assert out["0"][1] == out["1"][1]
     assert np.array_equal(out["0"][2], out["1"][2])
+
+
+@pytest.mark.parametrize("tol", [1e-6, 0.0])
+def test_nonfinite_flow_stops_at_the_first_check(tol):
+    """A non-finite field is caught on the device at the first sampled mean
+    |u_x| (every 50 iterations) instead of running to the cap; the caller
+    sees the reference's SystemExit for non-finite fields.  The fault is
+    made on the host: a NaN driving force."""
+    from prtlb_gpu import stokes_d3q19, stokes_d2q9
+    z = load_golden("flow_spheres3d")
+    for fn, g in ((stokes_d3q19, z["g"]), (stokes_d2q9, load_golden("flow_disks2d")["g"])):
+        info = {}
+        with pytest.raises(SystemExit) as e, contextlib.redirect_stdout(io.StringIO()):
+            fn(g, nit=30000, force=float("nan"), tol=tol, info=info, precision="fp32")
+        assert "non-finite" in str(e.value)
+        assert info["flow_iters"] == 50 and not info["flow_converged"]
