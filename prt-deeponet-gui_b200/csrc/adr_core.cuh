@@ -118,9 +118,53 @@ __device__ __forceinline__ float ld_c(const float* __restrict__ Cj, int c, int x
     return (pin && x == 0) ? feed : v;
 }
 
-// transport() of one chemical at one voxel (prtlb_3d.py:1182-1208).  BF:
-// the run has biofilm; without it no voxel carries a biofilm flag, every
-// face takes the pore diffusivity, and the biofilm count is not formed.
+// One axis of transport() at one voxel (prtlb_3d.py:1182-1208), from the
+// four neighbour values along the axis (clamped positions, inlet feed already
+// applied), the two face velocities and the voxel's flags: adds the axis'
+// diffusion and advection to `out` and its velocity difference to `divu`, in
+// the reference's operation order.  BF: the run has biofilm; without it no
+// voxel carries a biofilm flag, every face takes the pore diffusivity, and
+// the biofilm count is not formed.  Every transport kernel calls this, so
+// they compute the same function bit for bit.
+template <bool BF>
+__device__ __forceinline__ void transport_axis(float& out, float& divu, float Cc, float vm1,
+                                               float vm2, float vp1, float vp2, float uL,
+                                               float uH, uint32_t fl, int a,
+                                               const float (&dj)[3]) {
+    const bool oL = fl & f_open_lo(a), oH = fl & f_open_hi(a);
+    const bool fL = fl & f_far_lo(a), fH = fl & f_far_hi(a);
+    const float Cm1 = oL ? vm1 : Cc;
+    const float Cp1 = oH ? vp1 : Cc;
+    const float Cm2 = fL ? vm2 : Cm1;
+    const float Cp2 = fH ? vp2 : Cp1;
+    float DL, DH;
+    if constexpr (BF) {
+        const int bf = (fl & F_BF) ? 1 : 0;
+        // face diffusivity by the biofilm count of its two voxels (0, 1,
+        // 2); selected, not indexed, so the table stays in registers
+        const int nl = bf + ((fl & f_nbf_lo(a)) ? 1 : 0);
+        const int nh = bf + ((fl & f_nbf_hi(a)) ? 1 : 0);
+        DL = oL ? (nl == 0 ? dj[0] : (nl == 1 ? dj[1] : dj[2])) : 0.f;
+        DH = oH ? (nh == 0 ? dj[0] : (nh == 1 ? dj[1] : dj[2])) : 0.f;
+    } else {
+        DL = oL ? dj[0] : 0.f;
+        DH = oH ? dj[0] : 0.f;
+    }
+    // out += D_hi (C+1 - C) + D_lo (C-1 - C)
+    out = out + (DH * (Cp1 - Cc) + DL * (Cm1 - Cc));
+    // upwind face values: the stencil is chosen first and limited once
+    // (the same function of the same three values as choosing between
+    // the two limited candidates)
+    const bool rH = uH >= 0.f, rL = uL >= 0.f;
+    const float fh = muscl(rH ? Cc : Cp1, rH ? Cm1 : Cp2, rH ? Cp1 : Cc);
+    const float flo = muscl(rL ? Cm1 : Cc, rL ? Cm2 : Cp1, rL ? Cc : Cm1);
+    // out -= u_hi f_hi - u_lo f_lo
+    out = out - (uH * fh - uL * flo);
+    divu = divu + (uH - uL);
+}
+
+// transport() of one chemical at one voxel (prtlb_3d.py:1182-1208), loading
+// its neighbours and faces from global memory (the compacted-list kernels).
 template <int ND, bool BF>
 __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, const Grid& g,
                                                const VoxelPos& v, uint32_t fl,
@@ -134,8 +178,6 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
         const int p = v.p[a];
         const int n = extent(g, a);
         const int s = stride(g, a);
-        const bool oL = fl & f_open_lo(a), oH = fl & f_open_hi(a);
-        const bool fL = fl & f_far_lo(a), fH = fl & f_far_hi(a);
         // clamped (edge-replicated) neighbour positions
         const int pm1 = p > 0 ? p - 1 : 0, pm2 = p > 1 ? p - 2 : 0;
         const int pp1 = p < n - 1 ? p + 1 : n - 1, pp2 = p < n - 2 ? p + 2 : n - 1;
@@ -151,34 +193,7 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
         const int fi = face_lo(g, v, a);
         const float uL = ld_early(face[a] + fi);
         const float uH = ld_early(face[a] + fi + face_step(g, a));
-        const float Cm1 = oL ? vm1 : Cc;
-        const float Cp1 = oH ? vp1 : Cc;
-        const float Cm2 = fL ? vm2 : Cm1;
-        const float Cp2 = fH ? vp2 : Cp1;
-        float DL, DH;
-        if constexpr (BF) {
-            const int bf = (fl & F_BF) ? 1 : 0;
-            // face diffusivity by the biofilm count of its two voxels (0, 1,
-            // 2); selected, not indexed, so the table stays in registers
-            const int nl = bf + ((fl & f_nbf_lo(a)) ? 1 : 0);
-            const int nh = bf + ((fl & f_nbf_hi(a)) ? 1 : 0);
-            DL = oL ? (nl == 0 ? dj[0] : (nl == 1 ? dj[1] : dj[2])) : 0.f;
-            DH = oH ? (nh == 0 ? dj[0] : (nh == 1 ? dj[1] : dj[2])) : 0.f;
-        } else {
-            DL = oL ? dj[0] : 0.f;
-            DH = oH ? dj[0] : 0.f;
-        }
-        // out += D_hi (C+1 - C) + D_lo (C-1 - C)
-        out = out + (DH * (Cp1 - Cc) + DL * (Cm1 - Cc));
-        // upwind face values: the stencil is chosen first and limited once
-        // (the same function of the same three values as choosing between
-        // the two limited candidates)
-        const bool rH = uH >= 0.f, rL = uL >= 0.f;
-        const float fh = muscl(rH ? Cc : Cp1, rH ? Cm1 : Cp2, rH ? Cp1 : Cc);
-        const float flo = muscl(rL ? Cm1 : Cc, rL ? Cm2 : Cp1, rL ? Cc : Cm1);
-        // out -= u_hi f_hi - u_lo f_lo
-        out = out - (uH * fh - uL * flo);
-        divu = divu + (uH - uL);
+        transport_axis<BF>(out, divu, Cc, vm1, vm2, vp1, vp2, uL, uH, fl, a, dj);
     }
     return out + Cc * divu;
 }
@@ -246,6 +261,36 @@ __device__ __forceinline__ void reaction(const float (&C)[NS], float surf,
     }
 }
 
+// The rest of step() at one solute voxel (prtlb_3d.py:1392-1413) once the
+// transport terms T of the moving chemicals are known: the reaction terms
+// (with the surface weight of a surface-only abiotic reaction), forward
+// Euler and the clip at zero.  C holds the voxel's values after the inlet
+// pin.
+template <int ND, int NS>
+__device__ __forceinline__ void adr_update(const float (&C)[NS], const float (&T)[NS], uint32_t fl,
+                                           const prt_adr_params& p, float (&cn)[NS]) {
+    float surf = 0.f;
+    if (p.abio_on && p.surface_only) {
+        float nface = 0.f;
+#pragma unroll
+        for (int i = 0; i < ND; ++i) {
+            const int a = Axes<ND>::ax(i);
+            nface = nface + ((fl & f_open_lo(a)) ? 0.f : 1.f);
+            nface = nface + ((fl & f_open_hi(a)) ? 0.f : 1.f);
+        }
+        surf = nface / (float)(2 * ND);
+    }
+    float dC[NS];
+    reaction<NS>(C, surf, p, dC);
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        const bool mv = (p.moving_mask >> j) & 1u;
+        const float rhs = mv ? (T[j] + dC[j]) : dC[j];
+        const float v = C[j] + p.dt * rhs;
+        cn[j] = np_max(v, 0.f);
+    }
+}
+
 // One transport step of solute voxel number kk (compacted C-order list) at
 // step n: reads the state after step n-1 from buf[(n-1)&1], writes the state
 // after step n to buf[n&1] and, when n is a snapshot step, to its ladder slot.
@@ -276,29 +321,14 @@ __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params&
                                      p.feed[j], dj);
         }
     }
-    float surf = 0.f;
-    if (p.abio_on && p.surface_only) {
-        float nface = 0.f;
-#pragma unroll
-        for (int i = 0; i < ND; ++i) {
-            const int a = Axes<ND>::ax(i);
-            nface = nface + ((fl & f_open_lo(a)) ? 0.f : 1.f);
-            nface = nface + ((fl & f_open_hi(a)) ? 0.f : 1.f);
-        }
-        surf = nface / (float)(2 * ND);
-    }
-    float dC[NS];
-    reaction<NS>(C, surf, p, dC);
+    float cn[NS];
+    adr_update<ND, NS>(C, T, fl, p, cn);
     const int slot = d.slot_of_step[n];
     float* __restrict__ lad = slot >= 0 ? d.ladder + (long long)slot * NS * N : nullptr;
 #pragma unroll
     for (int j = 0; j < NS; ++j) {
-        const bool mv = (p.moving_mask >> j) & 1u;
-        const float rhs = mv ? (T[j] + dC[j]) : dC[j];
-        float cn = C[j] + p.dt * rhs;
-        cn = np_max(cn, 0.f);
-        Cout[j * N + c] = cn;
-        if (lad) lad[j * N + c] = cn;
+        Cout[j * N + c] = cn[j];
+        if (lad) lad[j * N + c] = cn[j];
     }
 }
 
