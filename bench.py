@@ -6,8 +6,9 @@
 Workload (one "step" = one complete solve of the plain 3D case):
   64^3 periodic pack of solid spheres, radius U[4, 7], porosity 0.45, seed 0
   (synthetic stand-in for the reference's rock images);
-  D3Q19 TRT Stokes from rest, float32 populations (f - w, float64 collision,
-  float64 residual), force 2e-6, tau 0.8, run to a relative change of
+  D3Q19 TRT Stokes from rest, float32 populations (f - w) collided in
+  float32, float64 residual and integrals, force 2e-6, tau 0.8, run to a
+  relative change of
   mean |u_x| <= 1e-6 per 50 iterations;
   then transport of one Monod solute (Ks = 0.5) at Pe = 10, Da = 1 until the
   reference's stop rule is met (tol 2e-3), 5 snapshots.
@@ -68,9 +69,14 @@ ADR_STEPS = None  # None: run to the reference's stop rule
 # instead of the voxel map because its working set fits in L2.
 TRAFFIC_PER_LAUNCH = {64: 25157632, 128: 176652032}
 PE, DA, KS, N_T = 10.0, 1.0, 0.5, 5
+# float32 populations collided in float32 (the "fp32" mode keeps the
+# momentum in float64); float64 only for the residual and the integrals
+PRECISION = "fp32f"
 METRIC = "D3Q19 TRT+ADR GLUPS"
 UNIT = "GLUPS"
 LB_BYTES_PER_FLUID = 19 * 4 * 2  # float32 populations read + written
+# one solute: C read and written, three face velocities, flags, list index
+ADR_BYTES_PER_SOLUTE = 4 + 4 + 12 + 4 + 4
 WORKLOAD = ("plain-3d: 64^3 sphere pack (r U[4,7], porosity 0.45, seed 0), D3Q19 TRT fp32 "
             "to tol 1e-6 + Monod ADR (Ks 0.5) Pe 10 Da 1 to the stop rule")
 
@@ -177,7 +183,7 @@ def device_solve(ctx, L, d_mat, d_vel, d_out, shape, chem):
     for i in range(3):
         p.dims[i] = shape[i]
     p.nit, p.force, p.tau, p.magic, p.tol = FLOW_NIT, FORCE, TAU, 3.0 / 16.0, FLOW_TOL
-    p.every, p.precision = 50, _lib.PRT_FP32
+    p.every, p.precision = 50, _lib.PRT_FP32_F32
     fi = _lib.FlowInfo()
     ctx.check(L.prt_flow_dev(ctx.handle, ctypes.c_void_p(d_mat), ctypes.byref(p),
                              ctypes.c_void_p(d_vel), ctypes.byref(fi)))
@@ -276,7 +282,7 @@ def run_ours(args, rank, world, torch, dist):
             e0.record(stream)
             w0 = time.perf_counter()
             v = stokes_d3q19(g, nit=FLOW_NIT, force=FORCE, tau_lb=TAU, tol=FLOW_TOL,
-                             precision="fp32", ctx=ctx)
+                             precision=PRECISION, ctx=ctx)
             w1 = time.perf_counter()
             tf = ctx.timing()
             out, tn = solve_adr(g, v, pe=PE, da=DA, n_t=N_T, n_species=1, chem=chem, ctx=ctx,
@@ -301,21 +307,90 @@ def run_ours(args, rank, world, torch, dist):
     lb_bytes = nfluid * LB_BYTES_PER_FLUID + 4 * ncell
     achieved = lb_bytes / (per_launch_ms * 1e-3) / 1e9
     peak, kind = peaks()
-    roof = {"kernel": "lb_step_kernel<D3Q19,ModeF32D>", "bound": "hbm",
+    roof = {"kernel": "lb_step_kernel<D3Q19,ModeF32>", "bound": "hbm",
+            "regime": "L2-resident (two lattices + slot table = 26 MB < 126 MB L2): "
+                      "latency-bound, not DRAM-bound; see side.dram_128 for the "
+                      "DRAM-resident figures",
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": kind,
-            "bytes_per_launch": lb_bytes, "traffic": TRAFFIC_PER_LAUNCH.get(EDGE),
+            "bytes_per_iteration": lb_bytes, "traffic": TRAFFIC_PER_LAUNCH.get(EDGE),
             "note": "algorithmic bytes = 152 B per pore voxel (19 float32 read + written) + "
-                    "4 B voxel map per voxel; per-launch time = flow loop events / "
-                    "iterations (includes graph node gaps and the convergence check); at "
-                    "this size the kernel reads a 72 B per pore voxel upstream-slot table "
-                    "from L2 instead of the map (traffic is a cold-cache capture)"}
+                    "4 B voxel map per voxel, per iteration; time per iteration = flow loop "
+                    "events / iterations (one launch per iteration, graph node gaps "
+                    "included); traffic = DRAM bytes of one cold-cache iteration (the slot "
+                    "table read instead of the map)"}
     res = {"ms_per_step": total_ms / args.steps, "value": value, "e2e": e2e_value,
            "h2d": h2d, "d2h": d2h, "launches": launches, "roof": roof, "clocks": clk.summary(),
            "flow_ms": fl_ms, "adr_ms": ad_ms, "iters": iters[0], "adr_steps": nsteps[0],
            "ncell": ncell, "nfluid": nfluid, "e2e_ms": e2e_ms, "e2e_split": e2e_split}
+    if rank == 0 and not args.no_side:
+        res["side"] = side_measurements(ctx, peak, kind)
     ctx.close()
     return res
+
+
+def side_measurements(ctx, peak, kind):
+    """Figures beside the bench line, each from its own loop's CUDA events:
+    the flow and transport kernels on a DRAM-resident 128^3 pack (porosity
+    0.45, seed 0: 2000 float32 flow iterations, 3000 Monod steps), and the
+    whole plain 2D configuration (128^2 disks, porosity 0.6, D2Q9 to tol 1e-7
+    at force 1e-6, then 4000 first-order steps at Pe 10, Da 1)."""
+    from prtlb_gpu import solve_adr, stokes_d2q9, stokes_d3q19
+    from prtlb_gpu.chemistry import default_chemistry, monod_chemistry
+    from prtlb_gpu.geometry import disk_pack_2d, sphere_pack_3d
+    quiet = contextlib.redirect_stdout(io.StringIO())
+    g = sphere_pack_3d(128, POROSITY, SEED)
+    n = int(g.size)
+    nf = int((g == 2).sum())
+    with quiet:
+        v = stokes_d3q19(g, nit=2000, tol=0.0, precision=PRECISION, ctx=ctx)
+        tf = ctx.timing()
+        solve_adr(g, v, pe=PE, da=DA, n_t=3, n_species=1, chem=monod_chemistry(KS), steps=3000,
+                  ctx=ctx)
+        ta = ctx.timing()
+    fl_us = tf[0] / tf[1] * 1e3
+    fl_bytes = nf * LB_BYTES_PER_FLUID + 4 * n
+    ad_us = ta[2] / ta[3] * 1e3
+    ad_bytes = nf * ADR_BYTES_PER_SOLUTE
+    dram = {
+        "workload": "128^3 sphere pack (r U[4,7], porosity 0.45, seed 0), %d pore voxels" % nf,
+        "flow": {"kernel": "lb_step_kernel<D3Q19,ModeF32>", "bound": "hbm",
+                 "us_per_iteration": round(fl_us, 3),
+                 "achieved": round(fl_bytes / fl_us / 1e3, 1), "peak": peak, "unit": "GB/s",
+                 "frac": round(fl_bytes / fl_us / 1e3 / peak, 4), "peak_kind": kind,
+                 "bytes_per_launch": fl_bytes, "traffic": TRAFFIC_PER_LAUNCH.get(128),
+                 "glups_all_voxels": round(n / fl_us / 1e3, 3),
+                 "glups_pore_voxels": round(nf / fl_us / 1e3, 3)},
+        "transport": {"kernel": "adr_step_kernel<3,1,no biofilm>", "bound": "hbm",
+                      "us_per_step": round(ad_us, 3),
+                      "achieved": round(ad_bytes / ad_us / 1e3, 1), "peak": peak, "unit": "GB/s",
+                      "frac": round(ad_bytes / ad_us / 1e3 / peak, 4), "peak_kind": kind,
+                      "bytes_per_launch": ad_bytes,
+                      "note": "algorithmic bytes = 28 B per solute voxel (C read + written, "
+                              "3 faces, flags, index); the kernel is bounded by instruction "
+                              "issue, not DRAM"},
+    }
+    g2 = disk_pack_2d(128, 0.6, SEED)
+    n2 = int(g2.size)
+    with quiet:
+        w0 = time.perf_counter()
+        v2 = stokes_d2q9(g2, nit=30000, force=1e-6, tau_lb=0.8, tol=1e-7, precision=PRECISION,
+                         ctx=ctx)
+        t2f = ctx.timing()
+        solve_adr(g2, v2, pe=PE, da=DA, n_t=5, n_species=1, chem=default_chemistry(1),
+                  steps=4000, ctx=ctx)
+        w1 = time.perf_counter()
+        t2a = ctx.timing()
+    dev_ms = t2f[0] + t2a[2]
+    ups = (t2f[1] + t2a[3]) * n2
+    plain2d = {"workload": "plain 2D: 128^2 disks (r U[4,8], porosity 0.6, seed 0), D2Q9 TRT "
+                           "fp32 force 1e-6 tau 0.8 to tol 1e-7, then one first-order solute "
+                           "Pe 10 Da 1, 4000 steps, 5 snapshots",
+               "flow_iters": int(t2f[1]), "transport_steps": int(t2a[3]),
+               "device_ms": round(dev_ms, 3), "glups": round(ups / (dev_ms * 1e6), 3),
+               "e2e_ms": round((w1 - w0) * 1e3, 3),
+               "e2e_glups": round(ups / ((w1 - w0) * 1e9), 3)}
+    return {"dram_128": dram, "plain2d": plain2d}
 
 
 # ---------------------------------------------------------------------------
@@ -565,6 +640,10 @@ def main():
     ap.add_argument("--edge", type=int, default=64)
     ap.add_argument("--flow-nit", type=int, default=30000)
     ap.add_argument("--adr-steps", type=int, default=None)
+    ap.add_argument("--no-cpu", action="store_true",
+                    help="skip the CPU baseline sample (profiling runs)")
+    ap.add_argument("--no-side", action="store_true",
+                    help="skip the 128^3 kernel rooflines and the plain 2D figures")
     # solves-per-hour modes (each prints its own line; the default is the
     # plain 3D bench line)
     ap.add_argument("--mode", default="plain",
@@ -584,7 +663,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     config = {"workload": WORKLOAD, "edge": EDGE, "voxels": EDGE ** 3, "porosity": POROSITY,
-              "seed": SEED, "flow": "D3Q19 TRT fp32 (f-w), fp64 collide+residual",
+              "seed": SEED, "flow": "D3Q19 TRT: f-w stored and collided in float32, "
+                                    "float64 residual, mass and permeability sums",
               "transport": "Monod Ks 0.5, Pe 10, Da 1, n_t 5, stop rule tol 2e-3",
               "l2": "flushed (256 MB write) before every timed step",
               "parallelism": "replicas" if world > 1 else "single"}
@@ -620,7 +700,7 @@ def main():
     r = run_ours(args, rank, world, torch, dist)
     if rank == 0:
         cpu = None
-        if world == 1:
+        if world == 1 and not args.no_cpu:
             v, res, wall = cpu_baseline_line(1, args.cpu_its, args.cpu_steps)
             cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": "%d D3Q19 iterations + %d Monod transport steps of the 64^3 "
@@ -639,10 +719,13 @@ def main():
                            "voxels": r["ncell"], "pore_voxels": r["nfluid"],
                            "e2e_ms": r["e2e_ms"], "e2e_split": r["e2e_split"],
                            "solves_per_hour": 3.6e6 / r["ms_per_step"] * world,
+                           # the same updates counted over the pore voxels only
+                           "glups_pore_voxels": r["value"] * r["nfluid"] / r["ncell"],
                            # each loop on its own, over all voxels (one chemical)
                            "flow_glups": r["iters"] * r["ncell"] / max(r["flow_ms"] * 1e6, 1e-9),
                            "transport_gcell_species_per_s":
-                               r["adr_steps"] * r["ncell"] / max(r["adr_ms"] * 1e6, 1e-9)}}
+                               r["adr_steps"] * r["ncell"] / max(r["adr_ms"] * 1e6, 1e-9)},
+                "side": r.get("side")}
         print(json.dumps(line))
     if dist is not None:
         dist.barrier()

@@ -411,6 +411,14 @@ int prt_walk_from_plane(prt_ctx* ctx, const uint8_t* mat, int32_t nd, const int3
                         int32_t pore_code, int32_t axis, int32_t plane, int32_t* steps_out,
                         int64_t* n_reached, int64_t* n_pore);
 
+/* Material codes of a solid grid (label_materials, build_geometry_3d.py:
+ * 224-239): `solid` (host, one byte per voxel, nonzero = solid, nd 2 or 3,
+ * dims as in prt_flow_params) gives mat_out (host, uint8 per voxel) = 2 for
+ * pore, 1 for solid with a pore face neighbour (the bounce-back wall), 0 for
+ * the other solid.  Positions beyond the grid's faces count as solid. */
+int prt_label_materials(prt_ctx* ctx, const uint8_t* solid, int32_t nd, const int32_t* dims,
+                        uint8_t* mat_out);
+
 /* ------------------------------------------------------------------------
  * check_physics (prtlb_3d.py:1632-1843) on the device: the statistics its
  * rules read, reduced from snapshots out (n_t, ns, voxels) float32 on the

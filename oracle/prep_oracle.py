@@ -168,3 +168,24 @@ def keep_percolating_cluster(solid, x_in, x_out):
         return solid, -1
     keep = np.isin(lab, sorted(good))
     return ~keep, int((pore & ~keep).sum())
+
+
+def label_materials(solid):
+    """Material codes of a boolean solid grid: pore 2, solid with a pore face
+    neighbour 1 (the bounce-back wall), other solid 0.  Neighbours beyond the
+    grid's faces count as solid: nothing wraps (build_geometry_3d.py:224-239,
+    a padded dilation over the three axes)."""
+    solid = np.asarray(solid, bool)
+    pore = ~solid
+    touch = np.zeros_like(pore)
+    for ax in range(pore.ndim):
+        n = pore.shape[ax]
+        lo = [slice(None)] * pore.ndim
+        hi = [slice(None)] * pore.ndim
+        lo[ax], hi[ax] = slice(0, n - 1), slice(1, n)
+        touch[tuple(hi)] |= pore[tuple(lo)]  # the neighbour below is pore
+        touch[tuple(lo)] |= pore[tuple(hi)]  # the neighbour above is pore
+    g = np.full(pore.shape, SOLID, np.uint8)
+    g[solid & touch] = WALL
+    g[pore] = PORE
+    return g

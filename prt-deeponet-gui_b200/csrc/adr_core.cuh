@@ -165,7 +165,11 @@ __device__ __forceinline__ void transport_axis(float& out, float& divu, float Cc
 
 // transport() of one chemical at one voxel (prtlb_3d.py:1182-1208), loading
 // its neighbours and faces from global memory (the compacted-list kernels).
-template <int ND, bool BF>
+// INNER: the voxel is at least three planes from the inlet and two from
+// every other face of the grid, so no neighbour position needs clamping and
+// no neighbour lies on the inlet plane (no feed to substitute): the same
+// values from fewer instructions.
+template <int ND, bool BF, bool INNER = false>
 __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, const Grid& g,
                                                const VoxelPos& v, uint32_t fl,
                                                const float* const* __restrict__ face, float Cc,
@@ -175,21 +179,29 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
 #pragma unroll
     for (int i = 0; i < ND; ++i) {
         const int a = Axes<ND>::ax(i);
-        const int p = v.p[a];
-        const int n = extent(g, a);
         const int s = stride(g, a);
-        // clamped (edge-replicated) neighbour positions
-        const int pm1 = p > 0 ? p - 1 : 0, pm2 = p > 1 ? p - 2 : 0;
-        const int pp1 = p < n - 1 ? p + 1 : n - 1, pp2 = p < n - 2 ? p + 2 : n - 1;
-        const int x0 = v.p[0];
-        const int xm1 = (a == 0) ? pm1 : x0, xm2 = (a == 0) ? pm2 : x0;
-        const int xp1 = (a == 0) ? pp1 : x0, xp2 = (a == 0) ? pp2 : x0;
-        // all four neighbours and both faces are loaded before the flags
-        // choose among them (clamped addresses are always in the grid)
-        const float vm1 = ld_c(Cj, v.c + (pm1 - p) * s, xm1, pin, feed);
-        const float vp1 = ld_c(Cj, v.c + (pp1 - p) * s, xp1, pin, feed);
-        const float vm2 = ld_c(Cj, v.c + (pm2 - p) * s, xm2, pin, feed);
-        const float vp2 = ld_c(Cj, v.c + (pp2 - p) * s, xp2, pin, feed);
+        float vm1, vp1, vm2, vp2;
+        if constexpr (INNER) {
+            vm1 = ld_early(Cj + (v.c - s));
+            vp1 = ld_early(Cj + (v.c + s));
+            vm2 = ld_early(Cj + (v.c - 2 * s));
+            vp2 = ld_early(Cj + (v.c + 2 * s));
+        } else {
+            const int p = v.p[a];
+            const int n = extent(g, a);
+            // clamped (edge-replicated) neighbour positions
+            const int pm1 = p > 0 ? p - 1 : 0, pm2 = p > 1 ? p - 2 : 0;
+            const int pp1 = p < n - 1 ? p + 1 : n - 1, pp2 = p < n - 2 ? p + 2 : n - 1;
+            const int x0 = v.p[0];
+            const int xm1 = (a == 0) ? pm1 : x0, xm2 = (a == 0) ? pm2 : x0;
+            const int xp1 = (a == 0) ? pp1 : x0, xp2 = (a == 0) ? pp2 : x0;
+            // all four neighbours and both faces are loaded before the flags
+            // choose among them (clamped addresses are always in the grid)
+            vm1 = ld_c(Cj, v.c + (pm1 - p) * s, xm1, pin, feed);
+            vp1 = ld_c(Cj, v.c + (pp1 - p) * s, xp1, pin, feed);
+            vm2 = ld_c(Cj, v.c + (pm2 - p) * s, xm2, pin, feed);
+            vp2 = ld_c(Cj, v.c + (pp2 - p) * s, xp2, pin, feed);
+        }
         const int fi = face_lo(g, v, a);
         const float uL = ld_early(face[a] + fi);
         const float uH = ld_early(face[a] + fi + face_step(g, a));
@@ -291,18 +303,14 @@ __device__ __forceinline__ void adr_update(const float (&C)[NS], const float (&T
     }
 }
 
-// One transport step of solute voxel number kk (compacted C-order list) at
-// step n: reads the state after step n-1 from buf[(n-1)&1], writes the state
-// after step n to buf[n&1] and, when n is a snapshot step, to its ladder slot.
-template <int ND, int NS, bool BF = true>
-__device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params& p, long long n,
-                                          long long kk) {
-    const int c = d.idx[kk];
-    const uint32_t fl = d.flags[c];
+// step() at one solute voxel (see adr_voxel), its flags and position known.
+template <int ND, int NS, bool BF, bool INNER>
+__device__ __forceinline__ void adr_voxel_body(const AdrDev& d, const prt_adr_params& p,
+                                               long long n, int c, uint32_t fl,
+                                               const VoxelPos& v) {
     const int N = (int)d.g.n;
     const float* __restrict__ Cin = d.buf[(n - 1) & 1];
     float* __restrict__ Cout = d.buf[n & 1];
-    const VoxelPos v = voxel_pos(c, d.div_z, d.div_y);
     const bool x0 = fl & F_X0;
     float C[NS];
 #pragma unroll
@@ -317,8 +325,8 @@ __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params&
         if ((p.moving_mask >> j) & 1u) {
             const bool pin = (p.pinned_mask >> j) & 1u;
             const float dj[3] = {p.dface[j][0], p.dface[j][1], p.dface[j][2]};
-            T[j] = transport_one<ND, BF>(Cin + j * N, d.g, v, fl, d.face, C[j], pin,
-                                     p.feed[j], dj);
+            T[j] = transport_one<ND, BF, INNER>(Cin + j * N, d.g, v, fl, d.face, C[j], pin,
+                                                p.feed[j], dj);
         }
     }
     float cn[NS];
@@ -330,6 +338,25 @@ __device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params&
         Cout[j * N + c] = cn[j];
         if (lad) lad[j * N + c] = cn[j];
     }
+}
+
+// One transport step of solute voxel number kk (compacted C-order list) at
+// step n: reads the state after step n-1 from buf[(n-1)&1], writes the state
+// after step n to buf[n&1] and, when n is a snapshot step, to its ladder slot.
+// A warp whose voxels all lie inside the grid's interior (see transport_one)
+// takes the interior form; the two forms give the same bits.
+template <int ND, int NS, bool BF = true>
+__device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params& p, long long n,
+                                          long long kk) {
+    const int c = d.idx[kk];
+    const uint32_t fl = d.flags[c];
+    const VoxelPos v = voxel_pos(c, d.div_z, d.div_y);
+    const Grid& g = d.g;
+    const bool inner = v.p[0] >= 3 && v.p[0] <= g.nx - 3 &&
+                       (ND == 2 || (v.p[1] >= 2 && v.p[1] <= g.ny - 3)) && v.p[2] >= 2 &&
+                       v.p[2] <= g.nz - 3;
+    if (__all_sync(__activemask(), inner)) adr_voxel_body<ND, NS, BF, true>(d, p, n, c, fl, v);
+    else adr_voxel_body<ND, NS, BF, false>(d, p, n, c, fl, v);
 }
 
 // The check of the time loop at step `end` (prtlb_3d.py:1499-1543), in

@@ -108,11 +108,70 @@ __global__ void __launch_bounds__(kWalkThreads)
     if (threadIdx.x == 0 && nb) atomicAdd(counts + 1, (unsigned long long)nb);
 }
 
+// label_materials (build_geometry_3d.py:224-239): pore 2, solid with a
+// pore face neighbour 1, other solid 0; positions beyond the grid's faces
+// count as solid (no wrap).  One thread per voxel, six neighbour reads
+// through the cache; 2D grids are (nx, 1, ny).
+__global__ void label_materials_kernel(const uint8_t* __restrict__ solid, WalkGrid w,
+                                       uint8_t* __restrict__ out) {
+    const long long n = w.g.n;
+    const unsigned c = blockIdx.x * kWalkThreads + threadIdx.x;
+    if (c >= (unsigned)n) return;
+    if (!solid[c]) {
+        out[c] = 2;
+        return;
+    }
+    int x, y, z;
+    coords(c, w, x, y, z);
+    const Grid& g = w.g;
+    const int sy = g.nz, sx = g.ny * g.nz;
+    bool touch = false;
+    if (x > 0) touch |= !solid[c - sx];
+    if (x < g.nx - 1) touch |= !solid[c + sx];
+    if (y > 0) touch |= !solid[c - sy];
+    if (y < g.ny - 1) touch |= !solid[c + sy];
+    if (z > 0) touch |= !solid[c - 1];
+    if (z < g.nz - 1) touch |= !solid[c + 1];
+    out[c] = touch ? 1 : 0;
+}
+
 }  // namespace
 
 }  // namespace prt
 
 using namespace prt;
+
+extern "C" int prt_label_materials(prt_ctx* ctx, const uint8_t* solid, int32_t nd,
+                                   const int32_t* dims, uint8_t* mat_out) {
+    if (!ctx || !solid || !dims || !mat_out) return fail(ctx, PRT_E_INVALID, "null argument");
+    if (nd != 2 && nd != 3) return fail(ctx, PRT_E_INVALID, "nd must be 2 or 3");
+    for (int i = 0; i < nd; ++i)
+        if (dims[i] <= 0) return fail(ctx, PRT_E_INVALID, "grid dimensions must be positive");
+    const Grid g = make_grid(nd, dims);
+    if (g.n >= (1ll << 31))
+        return fail(ctx, PRT_E_INVALID, "grids of 2^31 voxels or more are not supported");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    PrepState& P = ctx->prep;
+    CK(P.mat.ensure((size_t)g.n * 2));  // the solid grid, then the codes
+    P.staged_mat = -1;
+    uint8_t* d_solid = P.mat.as<uint8_t>();
+    uint8_t* d_out = d_solid + g.n;
+    CK(cudaMemcpyAsync(d_solid, solid, (size_t)g.n, cudaMemcpyHostToDevice, s));
+    WalkGrid w;
+    w.g = g;
+    w.dz = make_fastdiv((unsigned)g.nz);
+    w.dy = make_fastdiv((unsigned)g.ny);
+    w.axis = 0;
+    w.plane = 0;
+    const unsigned nb = (unsigned)((g.n + kWalkThreads - 1) / kWalkThreads);
+    label_materials_kernel<<<nb, kWalkThreads, 0, s>>>(d_solid, w, d_out);
+    CK(cudaGetLastError());
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(mat_out, d_out, (size_t)g.n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return PRT_OK;
+}
 
 extern "C" int prt_walk_from_plane(prt_ctx* ctx, const uint8_t* mat, int32_t nd,
                                    const int32_t* dims, int32_t pore_code, int32_t axis,

@@ -133,6 +133,8 @@ _PROTOS = {
                                               ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                               ctypes.c_int32, ctypes.c_float,
                                               ctypes.POINTER(ctypes.c_float)]),
+    "prt_label_materials": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                           ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p]),
     "prt_walk_from_plane": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                            ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,

@@ -16,6 +16,8 @@ arguments and outputs:
   percolates_between,    build_geometry_3d.py:201-221 (_percolates and
   keep_percolating_cluster  keep_percolating_cluster: two walks, one from each
                          plane; a component touches both when both reach it)
+  label_materials        build_geometry_3d.py:224-239 (a face-neighbour
+                         stencil, no walk)
 
 The reference labels components with scipy and walks with a Python queue,
 one voxel at a time; here each level of the walk is one kernel launch over
@@ -229,3 +231,21 @@ def keep_percolating_cluster(solid, x_in, x_out, *, device=None, ctx=None):
     if not keep.any():
         return solid, -1
     return ~keep, int(n_pore - np.count_nonzero(keep))
+
+
+def label_materials(solid, *, device=None, ctx=None):
+    """Material codes of a boolean solid grid on the GPU: pore 2, solid with a
+    pore face neighbour 1 (the bounce-back wall), other solid 0; beyond the
+    grid's faces counts as solid, nothing wraps (label_materials,
+    build_geometry_3d.py:224-239).  2D and 3D grids."""
+    solid = np.ascontiguousarray(np.asarray(solid, bool).view(np.uint8))
+    if solid.ndim not in (2, 3):
+        raise ValueError("label_materials expects a 2D or 3D grid, got %dD" % solid.ndim)
+    ctx = ctx or _lib.default_context(device)
+    dims = (ctypes.c_int32 * 3)(*(list(solid.shape) + [1] * (3 - solid.ndim)))
+    out = np.empty(solid.shape, np.uint8)
+    with ctx.lock:
+        ctx.check(_lib.lib().prt_label_materials(ctx.handle, solid.ctypes.data_as(ctypes.c_void_p),
+                                                 solid.ndim, dims,
+                                                 out.ctypes.data_as(ctypes.c_void_p)))
+    return out

@@ -113,6 +113,17 @@ def main():
             arrays["geodesic_2d"] = np.asarray(bd2.geodesic_2d(np.asarray(kept)), np.float32)
             arrays["percolates"] = np.asarray(bd2.percolates(g))
         save(name, **arrays)
+    # label_materials (build_geometry_3d.py:224-239): the 3D grids above as
+    # solids, plus seeded solids whose pore touches every face of the box
+    rng = np.random.default_rng(11)
+    solids = {"label_site3d": grids()["prep_site3d"] != p3.PORE,
+              "label_dense3d": grids()["prep_site3d_dense"] != p3.PORE,
+              "label_rand3d": rng.random((17, 13, 9)) < 0.5,
+              "label_sparse3d": rng.random((9, 11, 16)) < 0.15,
+              "label_allsolid3d": np.ones((5, 4, 3), bool)}
+    for name, solid in solids.items():
+        save(name, solid=np.asarray(solid, bool),
+             materials=np.asarray(bg3.label_materials(np.asarray(solid, bool)), np.uint8))
 
 
 if __name__ == "__main__":

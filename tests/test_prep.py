@@ -191,3 +191,33 @@ def test_argument_checks_need_no_gpu():
     s = prep._seeded(0.1, 3)
     assert s.dtype == np.float32 and s[3] == ((np.float32(0.1) + np.float32(1)) + np.float32(1)) + \
         np.float32(1)
+
+
+LABEL = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "label_*.npz")))
+
+
+@pytest.mark.parametrize("name", LABEL)
+def test_label_materials_oracle_matches_reference(name):
+    from oracle import prep_oracle as O
+    z = load_golden(name)
+    assert _same(O.label_materials(z["solid"]), z["materials"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", LABEL)
+def test_label_materials_gpu_matches_reference(name):
+    from prtlb_gpu import prep
+    z = load_golden(name)
+    assert _same(prep.label_materials(z["solid"]), z["materials"])
+
+
+@pytest.mark.gpu
+def test_label_materials_gpu_matches_oracle_on_larger_grids():
+    """2D and 3D, sparse and dense solids, odd sizes (block tails)."""
+    from oracle import prep_oracle as O
+    from prtlb_gpu import prep
+    rng = np.random.default_rng(5)
+    for shape, p in (((97, 64, 33), 0.5), ((64, 64, 64), 0.85), ((130, 77), 0.4),
+                     ((1, 1, 5), 0.5), ((3, 200), 0.7)):
+        solid = rng.random(shape) < p
+        assert _same(prep.label_materials(solid), O.label_materials(solid)), shape
