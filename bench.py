@@ -424,8 +424,14 @@ def run_batched(args, torch):
     from prtlb_gpu import _lib
     from prtlb_gpu.batch import solve_batch
     from prtlb_gpu.workloads import batched_set
+    from prtlb_gpu.workloads import request_set
     t = time.perf_counter()
-    reqs, draws = batched_set(args.requests, seed=SEED)
+    if args.edge_lo or args.edge_hi:
+        lo, hi = args.edge_lo or 24, args.edge_hi or 96
+        reqs, draws = request_set(args.requests, lo, hi, seed=SEED)
+    else:
+        lo, hi = 24, 96
+        reqs, draws = batched_set(args.requests, seed=SEED)
     gen_s = time.perf_counter() - t
     small, _ = batched_set(2, seed=SEED + 1, nit=200, max_steps=200)
     ctx = _lib.Context(0)
@@ -443,21 +449,26 @@ def run_batched(args, torch):
         torch.cuda.synchronize()
         t_streams = time.perf_counter() - t0
         t0 = time.perf_counter()
-        ref = [plain_solve(r, ctx) for r in reqs]
+        ref, loops = [], []
+        for r in reqs:
+            ref.append(plain_solve(r, ctx))
+            loops.append(ctx.timing())
         torch.cuda.synchronize()
         t_plain = time.perf_counter() - t0
     ctx.close()
     n = len(reqs)
     same = all(_same(a, b) for a, b in zip(res, ref))
     cells = sum(int(r.mat.size) for r in reqs)
+    ceiling = batching_ceiling(reqs, loops, t_plain)
     return {"metric": "batched solves/h", "value": n / t_batch * 3600.0, "unit": "solves/h",
             "n_gpus": 1, "steps": 1, "warmup": args.warmup, "ms_per_step": t_batch * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "batched: %d sphere packs, edge U{24..96}, porosity U[0.35,0.6],"
-                                   " Pe logU[0.1,100], Da logU[0.01,10], kinetics Monod / first "
-                                   "order / reversible sorption, D3Q19 fp32 to tol 1e-6 (cap "
-                                   "30000) + ADR to the stop rule (cap 100000)" % n,
+            "config": {"workload": "batched: %d sphere packs, edge U{%d..%d}, porosity "
+                                   "U[0.35,0.6], Pe logU[0.1,100], Da logU[0.01,10], kinetics "
+                                   "Monod / first order / reversible sorption, D3Q19 fp32 to tol "
+                                   "1e-6 (cap 30000) + ADR to the stop rule (cap 100000)" % (
+                                       n, lo, hi),
                        "voxels": cells, "seed": SEED, "geometry_s": round(gen_s, 2)},
             "mode": "tiles: one persistent launch per class of solves per step over a work "
                     "list of 256-voxel tiles, K steps per CUDA graph, autotuned tiling",
@@ -465,7 +476,34 @@ def run_batched(args, torch):
             "streams": {"solves_per_hour": n / t_streams * 3600.0, "seconds": t_streams,
                         "identical_to_plain": all(_same(a, b) for a, b in zip(res_streams, ref))},
             "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": same,
+            "ceiling": ceiling,
             "failed": sum(1 for r in res if r.error is not None), "clocks": clk.summary()}
+
+
+def batching_ceiling(reqs, loops, t_plain):
+    """What any batching of these solves can gain at most: the plain solves'
+    wall time against the time their algorithmic bytes take at the HBM peak
+    (flow: 2 x 19 float32 populations per pore voxel and iteration plus the
+    4-byte voxel map; transport: (8 ns + 20) bytes per solute voxel and
+    step), and against the sum of their device loops alone."""
+    peak, kind = peaks()
+    es = {"fp64": 8, "fp32": 4, "fp32f": 4, "fp16": 2}
+    t_bytes = t_loops = 0.0
+    for r, tm in zip(reqs, loops):
+        nf = int((np.asarray(r.mat) == 2).sum())
+        nv = int(np.asarray(r.mat).size)
+        ns = int(r.adr["n_species"])
+        fb = tm[1] * (2 * 19 * es[r.flow["precision"]] * nf + 4 * nv)
+        ab = tm[3] * (8 * ns + 20) * nf
+        t_bytes += (fb + ab) / (peak * 1e9)
+        t_loops += (tm[0] + tm[2]) * 1e-3
+    return {"plain_wall_s": t_plain, "plain_device_loops_s": t_loops,
+            "bytes_at_peak_s": t_bytes, "peak_gbs": peak, "peak_kind": kind,
+            "max_speedup_bytes": t_plain / max(t_bytes, 1e-12),
+            "max_speedup_host_overhead": t_plain / max(t_loops, 1e-12),
+            "note": "a batch can at most remove the host and launch time between loops "
+                    "(max_speedup_host_overhead) and, beyond that, make every loop run at "
+                    "the HBM peak on algorithmic bytes (max_speedup_bytes)"}
 
 
 def run_served(args, torch):
@@ -650,6 +688,10 @@ def main():
                     choices=["plain", "batched", "served", "precision"])
     ap.add_argument("--adr-sweep-steps", type=int, default=3000)
     ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--edge-lo", type=int, default=0,
+                    help="batched mode: smallest cubic edge (default: the batched set's 24)")
+    ap.add_argument("--edge-hi", type=int, default=0,
+                    help="batched mode: largest cubic edge (default: the batched set's 96)")
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--serve-mode", default="streams", choices=["streams", "tiles"])
     ap.add_argument("--flow-cap", type=int, default=2000000)

@@ -26,8 +26,14 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
     using S = typename M::S;
     __shared__ int s_last;
     __shared__ __align__(16) FlowJob sj;  // the tile's job: constants read where they are used
+    // programmatic dependent launch: the work list and the job descriptors
+    // are not written inside the graph, so the first tile's descriptor is
+    // copied while the previous step drains; control blocks and lattices
+    // are touched only after griddepcontrol.wait
+    griddep_launch_dependents();
     int t0, t1, cur = -1;
     tile_range(*ntiles_p, t0, t1);
+    bool waited = false;
     for (int t = t0; t < t1; ++t) {
         const BatchTile tl = tiles[t];
         if (tl.job != cur) {  // uniform over the block
@@ -35,6 +41,10 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
             cur = tl.job;
         }
         __syncthreads();
+        if (!waited) {  // uniform over the block
+            griddep_wait();
+            waited = true;
+        }
         FlowCtrl* ctrl = sj.ctrl;
         const long long it = __ldcg(&ctrl->it_base);
         const bool run = !__ldcg(&ctrl->done) && it < __ldcg(&ctrl->nit);
@@ -77,8 +87,16 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
 template <class L, class M>
 static cudaError_t launch_batch_t(const FlowJob* jobs, const BatchTile* tiles, const int* ntiles,
                                   int grid, cudaStream_t s) {
-    batch_flow_kernel<L, M><<<grid, kFlowThreads, 0, s>>>(jobs, tiles, ntiles);
-    return cudaGetLastError();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kFlowThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, batch_flow_kernel<L, M>, jobs, tiles, ntiles);
 }
 
 template <class L, class M>

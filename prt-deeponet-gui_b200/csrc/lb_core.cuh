@@ -4,6 +4,8 @@
 
 #include <cuda_fp16.h>
 
+#include <cstdlib>
+
 #include "prt_internal.h"
 
 namespace prt {
@@ -214,6 +216,13 @@ __device__ __forceinline__ void griddep_launch_dependents() {
     asm volatile("griddepcontrol.launch_dependents;" :::);
 }
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Whether flow step launches (single solves and batches) carry the
+// programmatic-serialisation attribute; PRT_PDL=0 launches them plainly.
+inline bool pdl_enabled() {
+    const char* v = std::getenv("PRT_PDL");
+    return !(v && v[0] == '0');
+}
 
 // 128-thread blocks: at 64^3 (458 blocks of 256 for 148 SMs) finer blocks
 // balance the SMs better and cut an iteration from 6.25 to 5.73 us.

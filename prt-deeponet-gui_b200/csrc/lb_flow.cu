@@ -217,16 +217,12 @@ __global__ void nbr_fill_kernel(FlowMap fm, Grid g, int* __restrict__ nbr) {
 // -------------------------------------------------------------------------
 int flow_blocks(long long n) { return (int)((n + kFlowThreads - 1) / kFlowThreads); }
 
-// Step kernels go out with programmatic stream serialisation: kernel t+1
-// starts launching while kernel t drains, reads its upstream slots (the maps
-// do not change during a solve) and waits in griddepcontrol.wait for t's
-// results.  Measured on the B200 with 128-thread blocks: 64^3 float32 4.89 ->
-// 4.82 us per iteration, float16 4.43 -> 4.18, 128^3 float32 41.3 -> 40.6.
-// PRT_PDL=0 launches them plainly.
-static bool pdl_enabled() {
-    const char* v = std::getenv("PRT_PDL");
-    return !(v && v[0] == '0');
-}
+// Step kernels go out with programmatic stream serialisation (pdl_enabled,
+// lb_core.cuh): kernel t+1 starts launching while kernel t drains, reads its
+// upstream slots (the maps do not change during a solve) and waits in
+// griddepcontrol.wait for t's results.  Measured on the B200 with 128-thread
+// blocks: 64^3 float32 4.89 -> 4.82 us per iteration, float16 4.43 -> 4.18,
+// 128^3 float32 41.3 -> 40.6.
 
 template <class L, class M, bool ODD, bool CHECK>
 static cudaError_t launch_step_one(typename M::S* f, const FlowMap& fm, const Grid& g,
