@@ -15,7 +15,8 @@ from .chemistry import (Chemistry, Sorption, default_chemistry,  # noqa: F401
                         reversible_sorption_chemistry)
 from .flow import permeability, stokes_d2q9, stokes_d3q19, trt_minus  # noqa: F401
 from .geometry import (assert_finite_distance, coat_with_biofilm,  # noqa: F401
-                       keep_inlet_connected, random_pack, sphere_pack_3d, disk_pack_2d)
+                       random_pack, sphere_pack_3d, disk_pack_2d)
+from .prep import keep_inlet_connected  # noqa: F401  (the GPU walk)
 from .physics import check_physics  # noqa: F401
 from . import prep  # noqa: F401  (the inlet walk on the GPU: keep_inlet_connected, geodesic_steps, ...)
 

@@ -1,10 +1,12 @@
-"""Host-side geometry: the reference's mask helpers and seeded synthetic packs.
+"""Host-side geometry: seeded synthetic packs and the mask helpers they need.
 
-keep_inlet_connected, coat_with_biofilm and assert_finite_distance restate
-3D/tools/prtlb_3d.py:530-612 (same inputs, outputs and messages).  The
-random disk / sphere packs are this project's own generators for the
+The random disk / sphere packs are this project's own generators for the
 benchmark workloads; the reference's build_spheres (build_geometry_3d.py:129)
-makes a different, walled geometry and is not reused.
+makes a different, walled geometry and is not reused.  The helpers below keep
+the outputs and messages of the reference's (prtlb_3d.py:530-612) for callers
+without a GPU, such as the pack generators; with a device,
+prtlb_gpu.keep_inlet_connected is the GPU walk (prtlb_gpu.prep), which gives
+the same grid bit for bit.
 """
 
 import numpy as np
@@ -12,58 +14,61 @@ import numpy as np
 SOLID, WALL, PORE = 0, 1, 2
 
 
-def keep_inlet_connected(g):
-    """Pore voxels not connected to the x = 0 face become solid.
-
-    Returns (g, n_removed); the inlet-touching components are kept, not the
-    largest one (prtlb_3d.py:530-563)."""
+def keep_inlet_connected_host(g):
+    """Pore voxels outside every face-connected pore component that touches
+    the x = 0 face become SOLID; returns (g, n_removed).  A grid with pore
+    but none of it on that face comes back unchanged with n_removed = the
+    pore count (the reference's behaviour, prtlb_3d.py:530-563)."""
     from scipy import ndimage
     g = np.asarray(g)
-    pore = (g == PORE)
+    pore = g == PORE
     if not pore.any():
         return g, 0
-    lab, _ = ndimage.label(pore)
-    seeds = np.unique(lab[0][pore[0]])
-    seeds = seeds[seeds != 0]
-    if seeds.size == 0:
+    labels, n = ndimage.label(pore)
+    on_face = np.zeros(n + 1, bool)  # component id -> touches x = 0
+    on_face[labels[0][pore[0]]] = True
+    on_face[0] = False
+    if not on_face.any():
         return g, int(pore.sum())
-    drop = pore & ~np.isin(lab, seeds)
-    if not drop.any():
+    cut = pore & ~on_face[labels]
+    n_cut = int(np.count_nonzero(cut))
+    if n_cut == 0:
         return g, 0
-    g = g.copy()
-    g[drop] = SOLID
-    return g, int(drop.sum())
+    out = g.copy()
+    out[cut] = SOLID
+    return out, n_cut
 
 
 def coat_with_biofilm(g, code, layers=1):
-    """Pore voxels within `layers` dilation steps of the rock get material
-    `code`.  Returns (g, n_marked) (prtlb_3d.py:566-592)."""
+    """Pore voxels within `layers` face-neighbour steps of non-pore become
+    material `code`; returns (g, n_marked) (prtlb_3d.py:566-592)."""
     from scipy import ndimage
     g = np.asarray(g).copy()
     if code is None or layers <= 0:
         return g, 0
-    grown = (g != PORE)
-    for _ in range(int(layers)):
-        grown = ndimage.binary_dilation(grown)
-    lining = grown & (g == PORE)
+    near = ndimage.binary_dilation(g != PORE, iterations=int(layers))
+    lining = near & (g == PORE)
     g[lining] = code
-    return g, int(lining.sum())
+    return g, int(np.count_nonzero(lining))
 
 
 def assert_finite_distance(d, g, name="geodesic"):
-    """None when `d` is finite (and < 1e6) on every pore voxel, else the
-    complaint (prtlb_3d.py:595-612)."""
-    d = np.asarray(d)
-    m = (np.asarray(g) == PORE)
-    if not m.any():
+    """None when the distance field `d` is finite and below 1e6 on every pore
+    voxel of `g`, else the reference's complaint (prtlb_3d.py:595-612); its
+    count adds the non-finite values and those >= 1e6, so an infinity counts
+    twice, as there."""
+    pore = np.asarray(g) == PORE
+    if not pore.any():
         return None
-    v = d[m]
-    if np.isfinite(v).all() and float(v.max()) < 1e6:
+    vals = np.asarray(d)[pore]
+    nonfinite = ~np.isfinite(vals)
+    huge = vals >= 1e6
+    if not (nonfinite.any() or huge.any()):
         return None
-    n = int((~np.isfinite(v)).sum() + (v >= 1e6).sum())
+    n = int(np.count_nonzero(nonfinite) + np.count_nonzero(huge))
     return ("%s is not finite on %d of %d pore voxels (max %.4g). Those voxels cannot be "
             "reached from the inlet; run keep_inlet_connected first."
-            % (name, n, m.sum(), float(v.max())))
+            % (name, n, pore.sum(), float(vals.max())))
 
 
 def _stamp(solid, centre, r, periodic=True):
@@ -136,7 +141,7 @@ def random_pack(shape, porosity, rmin, rmax, seed=0, max_tries=None, overlap_aft
     loop = _pack_loop_native if native else _pack_loop_numpy
     solid = loop(shape, porosity, rmin, rmax, seed, max_tries, overlap_after)
     g = np.where(solid, SOLID, PORE).astype(np.uint8)
-    g, _ = keep_inlet_connected(g)
+    g, _ = keep_inlet_connected_host(g)
     return g
 
 

@@ -5,5 +5,6 @@ from . import SOLID, WALL, PORE  # noqa: F401
 from .adr import solve_adr, _wanted_steps, _nearest_unused  # noqa: F401
 from .chemistry import Chemistry, default_chemistry  # noqa: F401
 from .flow import stokes_d3q19, trt_minus as _trt_minus  # noqa: F401
-from .geometry import assert_finite_distance, coat_with_biofilm, keep_inlet_connected  # noqa: F401
+from .geometry import assert_finite_distance, coat_with_biofilm  # noqa: F401
+from .prep import keep_inlet_connected  # noqa: F401
 from .physics import check_physics  # noqa: F401

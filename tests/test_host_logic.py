@@ -70,7 +70,7 @@ def test_abiotic_without_reactant_is_refused():
 def test_geometry_helpers():
     g = np.full((10, 6, 6), 2, np.uint8)
     g[4] = 0
-    g2, n = G.keep_inlet_connected(g)
+    g2, n = G.keep_inlet_connected_host(g)
     assert n == 5 * 36 and (g2[5:] == 0).all()
     gb, nb = G.coat_with_biofilm(np.pad(np.full((6, 6), 2, np.uint8), 1), 3, 1)
     assert nb > 0 and (gb == 3).sum() == nb
