@@ -158,15 +158,6 @@ __device__ __forceinline__ void upstream_slots(const FlowMap& fm, const Grid& g,
     }
 }
 
-// The same slots from the upstream-slot table fm.nbr (coalesced: entry i-1
-// of every slot is one contiguous row).
-template <class L>
-__device__ __forceinline__ void upstream_slots_table(const FlowMap& fm, int k, int (&src)[L::Q]) {
-    src[0] = k;
-#pragma unroll
-    for (int i = 1; i < L::Q; ++i) src[i] = __ldg(fm.nbr + (i - 1) * fm.nf + k);
-}
-
 // Gather the arrived populations of pore voxel number k (see the file
 // comment).  Lattices hold the pore voxels only, in C order: voxel
 // cells[k] is slot k, and imap[voxel] is the slot of a pore voxel or -1.
@@ -188,24 +179,44 @@ __device__ __forceinline__ Lat<S> lattices(S* f, int nf, bool odd) {
     return Lat<S>{f, odd ? qn : 0, odd ? 0 : qn, nf};
 }
 
+// The element offsets (into the two lattices) of the populations slot k
+// pulls in an iteration whose read lattice is `lat`: direction i from the
+// upstream slot src[i] of the read lattice, or, when that voxel is rock,
+// x's own value of two iterations back, opp(i) in the write lattice.
 template <class L, class S>
-__device__ __forceinline__ void gather_from_slots(const Lat<S>& lat, int k,
-                                                  const int (&src)[L::Q], float inv,
-                                                  typename Pop<S>::H (&h)[L::Q]) {
-    h[0] = Pop<S>::ld(lat.in(0, k), inv);
+__device__ __forceinline__ void pull_offsets(const Lat<S>& lat, int k, const int (&src)[L::Q],
+                                             int (&off)[L::Q]) {
+    off[0] = lat.rd + k;
 #pragma unroll
-    for (int i = 1; i < L::Q; ++i) {
-        // a rock upstream neighbour: x's own value of two iterations back
-        h[i] = Pop<S>::ld(src[i] >= 0 ? lat.in(i, src[i]) : lat.out(L::opp(i), k), inv);
-    }
+    for (int i = 1; i < L::Q; ++i)
+        off[i] = src[i] >= 0 ? lat.rd + i * lat.nf + src[i] : lat.wr + L::opp(i) * lat.nf + k;
+}
+
+// The same offsets from the pull tables fm.nbr, one per parity of the read
+// lattice (coalesced: entry i-1 of every slot is one contiguous row).
+template <class L, class S>
+__device__ __forceinline__ void pull_offsets_table(const FlowMap& fm, const Lat<S>& lat, int k,
+                                                   int (&off)[L::Q]) {
+    const int* tab = fm.nbr + (lat.rd != 0 ? (L::Q - 1) * fm.nf : 0);
+    off[0] = lat.rd + k;
+#pragma unroll
+    for (int i = 1; i < L::Q; ++i) off[i] = __ldg(tab + (i - 1) * fm.nf + k);
+}
+
+template <class L, class S>
+__device__ __forceinline__ void gather_from_offsets(const Lat<S>& lat, const int (&off)[L::Q],
+                                                    float inv, typename Pop<S>::H (&h)[L::Q]) {
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) h[i] = Pop<S>::ld(lat.f + off[i], inv);
 }
 
 template <class L, class S>
 __device__ __forceinline__ void gather(const Lat<S>& lat, int k, const FlowMap& fm, const Grid& g,
                                        float inv, typename Pop<S>::H (&h)[L::Q]) {
-    int src[L::Q];
+    int src[L::Q], off[L::Q];
     upstream_slots<L>(fm, g, k, src);
-    gather_from_slots<L, S>(lat, k, src, inv, h);
+    pull_offsets<L, S>(lat, k, src, off);
+    gather_from_offsets<L, S>(lat, off, inv, h);
 }
 
 // Programmatic dependent launch: let the next kernel in the stream start
@@ -251,19 +262,13 @@ struct Staged {
     __device__ S operator[](int i) const { return col[i * kFlowThreads]; }
 };
 
-// gather() with the population loads issued as cp.async into `col` (this
+// The gather with the population loads issued as cp.async into `col` (this
 // thread's column of a [Q][kFlowThreads] shared array): the same sources,
 // but no register is held while a load is in flight.
 template <class L, class S>
-__device__ __forceinline__ void gather_staged(const Lat<S>& lat, int k, const int (&src)[L::Q],
-                                              S* col) {
-    cp_async_pop(col, lat.in(0, k));
+__device__ __forceinline__ void gather_staged(const Lat<S>& lat, const int (&off)[L::Q], S* col) {
 #pragma unroll
-    for (int i = 1; i < L::Q; ++i) {
-        const int off = src[i] >= 0 ? lat.rd + i * lat.nf + src[i]
-                                    : lat.wr + L::opp(i) * lat.nf + k;
-        cp_async_pop(col + i * kFlowThreads, lat.f + off);
-    }
+    for (int i = 0; i < L::Q; ++i) cp_async_pop(col + i * kFlowThreads, lat.f + off[i]);
     cp_async_wait_all();
 }
 
@@ -340,40 +345,52 @@ __device__ __forceinline__ void collide_store(const Lat<S>& lat, int c, const HA
 }
 
 // One pore voxel (slot k) of one LB iteration from the read lattice into
-// the write lattice, its upstream slots already found: gather, moments,
-// collision, store; returns |u_x| for the convergence mean.
+// the write lattice, the offsets of its pulls already found: gather,
+// moments, collision, store; returns |u_x| for the convergence mean.
 template <class L, class M>
-__device__ __forceinline__ double lb_cell_slots(const Lat<typename M::S>& lat, const LbParams& kc,
-                                                int k, const int (&src)[L::Q]) {
+__device__ __forceinline__ double lb_cell_offs(const Lat<typename M::S>& lat, const LbParams& kc,
+                                               int k, const int (&off)[L::Q]) {
     using S = typename M::S;
     using R = typename M::R;
     using RA = typename M::RA;
     if constexpr (M::staged) {
         __shared__ S stage[L::Q * kFlowThreads];
         S* col = stage + threadIdx.x;
-        gather_staged<L, S>(lat, k, src, col);
+        gather_staged<L, S>(lat, off, col);
         const Staged<S> h{col};
         const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
         collide_store<L, S, R, RA>(lat, k, h, m, kc);
         return fabs((double)m.jx * (double)m.inv_rho);
     } else {
         typename Pop<S>::H h[L::Q];
-        gather_from_slots<L, S>(lat, k, src, kc.inv_scale, h);
+        gather_from_offsets<L, S>(lat, off, kc.inv_scale, h);
         const Moments<R, RA> m = moments<L, R, RA>(h, kc.half_g);
         collide_store<L, S, R, RA>(lat, k, h, m, kc);
         return fabs((double)m.jx * (double)m.inv_rho);
     }
 }
 
-// The same, finding the upstream slots first (from the slot table when the
-// solve has one: the same slots either way).
+// The offsets of slot k's pulls: from the pull tables when the solve has
+// them, else from the packed cell and the voxel map (the same offsets).
+template <class L, class S>
+__device__ __forceinline__ void find_pulls(const Lat<S>& lat, const FlowMap& fm, const Grid& g,
+                                           int k, int (&off)[L::Q]) {
+    if (fm.nbr) {
+        pull_offsets_table<L, S>(fm, lat, k, off);
+    } else {
+        int src[L::Q];
+        upstream_slots<L>(fm, g, k, src);
+        pull_offsets<L, S>(lat, k, src, off);
+    }
+}
+
+// The same, finding the pulls first.
 template <class L, class M>
 __device__ __forceinline__ double lb_cell_rw(const Lat<typename M::S>& lat, const FlowMap& fm,
                                              const Grid& g, const LbParams& kc, int k) {
-    int src[L::Q];
-    if (fm.nbr) upstream_slots_table<L>(fm, k, src);
-    else upstream_slots<L>(fm, g, k, src);
-    return lb_cell_slots<L, M>(lat, kc, k, src);
+    int off[L::Q];
+    find_pulls<L, typename M::S>(lat, fm, g, k, off);
+    return lb_cell_offs<L, M>(lat, kc, k, off);
 }
 
 // Block sum of one double per thread (warp shuffles, then the warp sums in

@@ -35,11 +35,13 @@ __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
                    const FlowCtrl* __restrict__ ctrl, int kstep, double* __restrict__ partials) {
     griddep_launch_dependents();
     const int k = blockIdx.x * kFlowThreads + threadIdx.x;
-    // the pore maps never change during a solve: the upstream slots are
-    // looked up while the previous iteration may still be running
-    int src[L::Q];
+    const Lat<typename M::S> lat = lattices<L>(f, fm.nf, ODD);
+    // the pore maps never change during a solve: the pulls (with tables) or
+    // the upstream slots (without) are looked up while the previous
+    // iteration may still be running
+    int off[L::Q], src[L::Q];
     if (k < fm.nf) {
-        if (fm.nbr) upstream_slots_table<L>(fm, k, src);
+        if (fm.nbr) pull_offsets_table<L>(fm, lat, k, off);
         else upstream_slots<L>(fm, g, k, src);
     }
     griddep_wait();
@@ -47,7 +49,8 @@ __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
     if (ctrl->done || it >= ctrl->nit) return;  // uniform over the grid
     double acc = 0.0;
     if (k < fm.nf) {
-        const double ux = lb_cell_slots<L, M>(lattices<L>(f, fm.nf, ODD), kc, k, src);
+        if (!fm.nbr) pull_offsets<L>(lat, k, src, off);
+        const double ux = lb_cell_offs<L, M>(lat, kc, k, off);
         if (CHECK) acc = ux;
     }
     if (CHECK) block_sum_store(acc, partials + blockIdx.x);
@@ -201,7 +204,8 @@ __global__ void imap_scatter_kernel(int* __restrict__ cells, int nf, int* __rest
     cells[k] = (int)(((unsigned)x << xs) | ((unsigned)y << ys) | (unsigned)z);
 }
 
-// The upstream-slot table: nbr[(i - 1) * nf + k] = upstream slot i of slot k.
+// The pull tables: for each parity p of the read lattice, nbr[p * (Q - 1) *
+// nf + (i - 1) * nf + k] = the element offset slot k pulls direction i from.
 template <class L>
 __global__ void nbr_fill_kernel(FlowMap fm, Grid g, int* __restrict__ nbr) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -209,7 +213,14 @@ __global__ void nbr_fill_kernel(FlowMap fm, Grid g, int* __restrict__ nbr) {
     int src[L::Q];
     upstream_slots<L>(fm, g, k, src);
 #pragma unroll
-    for (int i = 1; i < L::Q; ++i) nbr[(i - 1) * fm.nf + k] = src[i];
+    for (int p = 0; p < 2; ++p) {
+        const Lat<char> lat = lattices<L, char>(nullptr, fm.nf, p != 0);
+        int off[L::Q];
+        pull_offsets<L, char>(lat, k, src, off);
+        int* tab = nbr + p * (L::Q - 1) * fm.nf;
+#pragma unroll
+        for (int i = 1; i < L::Q; ++i) tab[(i - 1) * fm.nf + k] = off[i];
+    }
 }
 
 // -------------------------------------------------------------------------

@@ -135,12 +135,15 @@ struct PairTree {
 // voxel in C order, whose coordinates are packed in cells[k] as
 // x << xs | y << ys | z (so a kernel finds its neighbours with shifts and
 // masks instead of divisions); imap[voxel] is the slot of a pore voxel, -1
-// for rock.  nbr, when not null, is the table of upstream slots
-// nbr[(i - 1) * nf + k] = slot of voxel k - e_i or -1 (i = 1 .. Q-1): the
-// step kernel then reads them in one coalesced pass instead of the packed
-// cell and imap lookups (one dependent load fewer).  Set up for solves whose
-// lattices and table fit in half the L2 cache, where the latency of the
-// lookups, not the bytes of the table, bounds an iteration.
+// for rock.  nbr, when not null, holds the pull tables, one per parity p of
+// the read lattice: nbr[p * (Q-1) * nf + (i - 1) * nf + k] = the element
+// offset (into the two lattices) slot k pulls direction i from -- the
+// upstream slot of the read lattice, or slot k's own opp(i) of the write
+// lattice when that voxel is rock (i = 1 .. Q-1).  The step kernel then
+// reads them in one coalesced pass instead of the packed cell, the imap
+// lookups and the choice between the two lattices.  Set up for solves whose
+// lattices and tables fit in half the L2 cache, where the latency of the
+// lookups, not the bytes of the tables, bounds an iteration.
 struct FlowMap {
     int nf;
     const int* cells;
@@ -149,14 +152,14 @@ struct FlowMap {
     const int* nbr;
 };
 
-// Bytes of the upstream-slot table of nf pore voxels (Q-1 ints each).
-inline long long flow_nbr_bytes(int q, long long nf) { return (long long)(q - 1) * nf * 4; }
+// Bytes of the two pull tables of nf pore voxels (Q-1 ints each per parity).
+inline long long flow_nbr_bytes(int q, long long nf) { return 2ll * (q - 1) * nf * 4; }
 
 // Whether a solve with nf pore voxels and populations of es bytes gets the
-// upstream-slot table on a device with l2_bytes of L2: when the two
-// lattices and the table fit in half of it.
+// pull tables on a device with l2_bytes of L2: when the two lattices and one
+// table (an iteration reads one) fit in half of it.
 inline bool flow_use_nbr(int q, long long nf, long long es, long long l2_bytes) {
-    return nf > 0 && 2 * q * nf * es + flow_nbr_bytes(q, nf) <= l2_bytes / 2;
+    return nf > 0 && 2 * q * nf * es + flow_nbr_bytes(q, nf) / 2 <= l2_bytes / 2;
 }
 
 // Constants of one flow solve (the TRT rates of _trt_minus and the Guo
@@ -226,7 +229,7 @@ cudaError_t flow_launch_flags(const uint8_t* mat, long long n, int pore, uint8_t
 // packed coordinates of fm (imap must hold -1 everywhere before).
 cudaError_t flow_launch_imap(int* cells, int nf, int* imap, const Grid& g, int ys, int xs,
                              cudaStream_t s);
-// The upstream-slot table of fm (cells and imap ready) into nbr,
+// The pull tables of fm (cells and imap ready) into nbr,
 // flow_nbr_bytes(Q, fm.nf) bytes.
 cudaError_t flow_launch_nbr(int nd, const FlowMap& fm, const Grid& g, int* nbr, cudaStream_t s);
 cudaError_t flow_launch_final_reduce(const double* partials, int nblocks, double* out,
