@@ -169,10 +169,30 @@ __device__ __forceinline__ void transport_axis(float& out, float& divu, float Cc
 // every other face of the grid, so no neighbour position needs clamping and
 // no neighbour lies on the inlet plane (no feed to substitute): the same
 // values from fewer instructions.
+// The face velocities of one voxel, low and high face of each of its ND axes
+// (in Axes<ND> order).  They do not change during a run.
+struct VoxelFaces {
+    float lo[3], hi[3];
+};
+
+template <int ND>
+__device__ __forceinline__ VoxelFaces load_faces(const Grid& g, const VoxelPos& v,
+                                                 const float* const* __restrict__ face) {
+    VoxelFaces fc;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+        const int a = Axes<ND>::ax(i);
+        const int fi = face_lo(g, v, a);
+        fc.lo[i] = ld_early(face[a] + fi);
+        fc.hi[i] = ld_early(face[a] + fi + face_step(g, a));
+    }
+    return fc;
+}
+
 template <int ND, bool BF, bool INNER = false>
 __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, const Grid& g,
                                                const VoxelPos& v, uint32_t fl,
-                                               const float* const* __restrict__ face, float Cc,
+                                               const VoxelFaces& fc, float Cc,
                                                bool pin, float feed, const float (&dj)[3]) {
     float out = 0.f;
     float divu = 0.f;
@@ -195,17 +215,14 @@ __device__ __forceinline__ float transport_one(const float* __restrict__ Cj, con
             const int x0 = v.p[0];
             const int xm1 = (a == 0) ? pm1 : x0, xm2 = (a == 0) ? pm2 : x0;
             const int xp1 = (a == 0) ? pp1 : x0, xp2 = (a == 0) ? pp2 : x0;
-            // all four neighbours and both faces are loaded before the flags
-            // choose among them (clamped addresses are always in the grid)
+            // all four neighbours are loaded before the flags choose among
+            // them (clamped addresses are always in the grid)
             vm1 = ld_c(Cj, v.c + (pm1 - p) * s, xm1, pin, feed);
             vp1 = ld_c(Cj, v.c + (pp1 - p) * s, xp1, pin, feed);
             vm2 = ld_c(Cj, v.c + (pm2 - p) * s, xm2, pin, feed);
             vp2 = ld_c(Cj, v.c + (pp2 - p) * s, xp2, pin, feed);
         }
-        const int fi = face_lo(g, v, a);
-        const float uL = ld_early(face[a] + fi);
-        const float uH = ld_early(face[a] + fi + face_step(g, a));
-        transport_axis<BF>(out, divu, Cc, vm1, vm2, vp1, vp2, uL, uH, fl, a, dj);
+        transport_axis<BF>(out, divu, Cc, vm1, vm2, vp1, vp2, fc.lo[i], fc.hi[i], fl, a, dj);
     }
     return out + Cc * divu;
 }
@@ -307,7 +324,7 @@ __device__ __forceinline__ void adr_update(const float (&C)[NS], const float (&T
 template <int ND, int NS, bool BF, bool INNER>
 __device__ __forceinline__ void adr_voxel_body(const AdrDev& d, const prt_adr_params& p,
                                                long long n, int c, uint32_t fl,
-                                               const VoxelPos& v) {
+                                               const VoxelPos& v, const VoxelFaces& fc) {
     const int N = (int)d.g.n;
     const float* __restrict__ Cin = d.buf[(n - 1) & 1];
     float* __restrict__ Cout = d.buf[n & 1];
@@ -325,7 +342,7 @@ __device__ __forceinline__ void adr_voxel_body(const AdrDev& d, const prt_adr_pa
         if ((p.moving_mask >> j) & 1u) {
             const bool pin = (p.pinned_mask >> j) & 1u;
             const float dj[3] = {p.dface[j][0], p.dface[j][1], p.dface[j][2]};
-            T[j] = transport_one<ND, BF, INNER>(Cin + j * N, d.g, v, fl, d.face, C[j], pin,
+            T[j] = transport_one<ND, BF, INNER>(Cin + j * N, d.g, v, fl, fc, C[j], pin,
                                                 p.feed[j], dj);
         }
     }
@@ -340,23 +357,50 @@ __device__ __forceinline__ void adr_voxel_body(const AdrDev& d, const prt_adr_pa
     }
 }
 
-// One transport step of solute voxel number kk (compacted C-order list) at
-// step n: reads the state after step n-1 from buf[(n-1)&1], writes the state
-// after step n to buf[n&1] and, when n is a snapshot step, to its ladder slot.
-// A warp whose voxels all lie inside the grid's interior (see transport_one)
-// takes the interior form; the two forms give the same bits.
+// What one transport step needs of solute voxel number kk (compacted C-order
+// list) that does not change during a run: its voxel index, flags,
+// position and face velocities.
+struct VoxelSetup {
+    int c;
+    uint32_t fl;
+    VoxelPos v;
+    VoxelFaces fc;
+};
+
+template <int ND>
+__device__ __forceinline__ VoxelSetup voxel_setup(const AdrDev& d, long long kk) {
+    VoxelSetup s;
+    s.c = d.idx[kk];
+    s.fl = d.flags[s.c];
+    s.v = voxel_pos(s.c, d.div_z, d.div_y);
+    s.fc = load_faces<ND>(d.g, s.v, d.face);
+    return s;
+}
+
+// One transport step of a solute voxel at step n: reads the state after
+// step n-1 from buf[(n-1)&1], writes the state after step n to buf[n&1]
+// and, when n is a snapshot step, to its ladder slot.  A warp whose voxels
+// all lie inside the grid's interior (see transport_one) takes the interior
+// form; the two forms give the same bits.
 template <int ND, int NS, bool BF = true>
-__device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params& p, long long n,
-                                          long long kk) {
-    const int c = d.idx[kk];
-    const uint32_t fl = d.flags[c];
-    const VoxelPos v = voxel_pos(c, d.div_z, d.div_y);
+__device__ __forceinline__ void adr_voxel_step(const AdrDev& d, const prt_adr_params& p,
+                                               long long n, const VoxelSetup& s) {
     const Grid& g = d.g;
+    const VoxelPos& v = s.v;
     const bool inner = v.p[0] >= 3 && v.p[0] <= g.nx - 3 &&
                        (ND == 2 || (v.p[1] >= 2 && v.p[1] <= g.ny - 3)) && v.p[2] >= 2 &&
                        v.p[2] <= g.nz - 3;
-    if (__all_sync(__activemask(), inner)) adr_voxel_body<ND, NS, BF, true>(d, p, n, c, fl, v);
-    else adr_voxel_body<ND, NS, BF, false>(d, p, n, c, fl, v);
+    if (__all_sync(__activemask(), inner))
+        adr_voxel_body<ND, NS, BF, true>(d, p, n, s.c, s.fl, v, s.fc);
+    else
+        adr_voxel_body<ND, NS, BF, false>(d, p, n, s.c, s.fl, v, s.fc);
+}
+
+// The same for solute voxel number kk (compacted C-order list).
+template <int ND, int NS, bool BF = true>
+__device__ __forceinline__ void adr_voxel(const AdrDev& d, const prt_adr_params& p, long long n,
+                                          long long kk) {
+    adr_voxel_step<ND, NS, BF>(d, p, n, voxel_setup<ND>(d, kk));
 }
 
 // The check of the time loop at step `end` (prtlb_3d.py:1499-1543), in

@@ -4,8 +4,6 @@
 
 #include <cuda_fp16.h>
 
-#include <cstdlib>
-
 #include "prt_internal.h"
 
 namespace prt {
@@ -217,22 +215,6 @@ __device__ __forceinline__ void gather(const Lat<S>& lat, int k, const FlowMap& 
     upstream_slots<L>(fm, g, k, src);
     pull_offsets<L, S>(lat, k, src, off);
     gather_from_offsets<L, S>(lat, off, inv, h);
-}
-
-// Programmatic dependent launch: let the next kernel in the stream start
-// launching now, and wait until the previous one has finished and its
-// stores are visible (both no-ops for a kernel launched without the
-// programmatic-serialisation attribute).
-__device__ __forceinline__ void griddep_launch_dependents() {
-    asm volatile("griddepcontrol.launch_dependents;" :::);
-}
-__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
-// Whether flow step launches (single solves and batches) carry the
-// programmatic-serialisation attribute; PRT_PDL=0 launches them plainly.
-inline bool pdl_enabled() {
-    const char* v = std::getenv("PRT_PDL");
-    return !(v && v[0] == '0');
 }
 
 // 128-thread blocks: at 64^3 (458 blocks of 256 for 148 SMs) finer blocks

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <cmath>
+#include <cstdlib>
 
 #include "../../include/prtlb.h"
 
@@ -44,6 +45,24 @@ __device__ __forceinline__ unsigned fast_div(unsigned t, const FastDiv& f) {
     return (__umulhi(t, f.m) + t) >> f.s;
 }
 #endif
+
+#ifdef __CUDACC__
+// Programmatic dependent launch: let the next kernel in the stream start
+// launching now, and wait until the previous one has finished and its
+// stores are visible (both no-ops for a kernel launched without the
+// programmatic-serialisation attribute).
+__device__ __forceinline__ void griddep_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" :::);
+}
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+#endif
+
+// Whether step launches (flow, batched flow, transport) carry the
+// programmatic-serialisation attribute; PRT_PDL=0 launches them plainly.
+inline bool pdl_enabled() {
+    const char* v = std::getenv("PRT_PDL");
+    return !(v && v[0] == '0');
+}
 
 // Device-side state of FlowConvergence (prtlb_3d.py:168-252) for one solve.
 struct FlowCtrl {

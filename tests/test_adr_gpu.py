@@ -114,3 +114,19 @@ def test_buffers_kept_between_runs_hold_no_stale_values():
         assert np.array_equal(out, z["out"])
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("pdl", ["0", "1"])
+def test_transport_with_and_without_programmatic_launch(monkeypatch, pdl):
+    """The transport step goes out with programmatic dependent launch by
+    default (its voxel index, flags and face velocities are read while the
+    previous step drains) or plainly (PRT_PDL=0); both match the reference's
+    golden runs bit for bit."""
+    monkeypatch.setenv("PRT_PDL", pdl)
+    for name in ("adr_spheres3d_biofilm", "adr_spheres3d_ns4", "adr_disks2d_first",
+                 "adr_chan2d_capped"):
+        z = load_golden(name)
+        out, tn, info, prog = run(z, name)
+        assert np.array_equal(tn, z["t_norm"]), name
+        assert np.array_equal(prog, z["progress"]), name
+        assert np.array_equal(out, z["out"]), (name, float(np.abs(out - z["out"]).max()))
