@@ -416,7 +416,6 @@ extern "C" int prt_adr_stage_dev(prt_ctx* ctx, const uint8_t* d_mat, const float
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
     AdrState& A = ctx->adr;
-    A.graph.release();
     A.keep_steps.clear();
     A.slot_of_index.clear();
     A.begun = A.ran = false;
@@ -561,7 +560,6 @@ extern "C" int prt_adr_begin(prt_ctx* ctx, const prt_adr_params* p) {
                     "chemicals x voxels too large for the transport's 32-bit indices");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
-    A.graph.release();
     A.p = *p;
     const Grid g = A.d.g;
     const long long N = g.n;
@@ -703,6 +701,41 @@ static cudaError_t adr_emit(prt_ctx* ctx, cudaGraphConditionalHandle h, int use)
     return adr_launch_stop(A.d, dctrl, dmeans, h, use, ctx->stream);
 }
 
+// Everything the transport loop graph bakes into its nodes: the device
+// descriptor and parameters the step kernels take by value, the chunk length,
+// the buffers of the means and the stop rule, and the launch attribute.
+static std::vector<unsigned char> adr_graph_key(prt_ctx* ctx) {
+    AdrState& A = ctx->adr;
+    const void* ptrs[3] = {A.means.p, A.src_slot.p, A.ctrl.p};
+    const int ints[2] = {A.rp.check, pdl_enabled() ? 1 : 0};
+    std::vector<unsigned char> k(sizeof(AdrDev) + sizeof(prt_adr_params) + sizeof(ptrs) +
+                                 sizeof(ints));
+    unsigned char* q = k.data();
+    memcpy(q, &A.d, sizeof(AdrDev));
+    q += sizeof(AdrDev);
+    memcpy(q, &A.p, sizeof(prt_adr_params));
+    q += sizeof(prt_adr_params);
+    memcpy(q, ptrs, sizeof(ptrs));
+    q += sizeof(ptrs);
+    memcpy(q, ints, sizeof(ints));
+    return k;
+}
+
+// The loop graph of the set-up run: the cached one when the key matches
+// (back-to-back solves of one geometry and chemistry), else a new capture.
+static cudaError_t adr_graph(prt_ctx* ctx) {
+    AdrState& A = ctx->adr;
+    std::vector<unsigned char> key = adr_graph_key(ctx);
+    if (A.graph.exec && key == A.graph_key) return cudaSuccess;
+    A.graph_key.clear();
+    cudaError_t e = build_while_graph(ctx->stream, A.graph, [&](cudaGraphConditionalHandle h,
+                                                                int use) {
+        return adr_emit(ctx, h, use);
+    });
+    if (e == cudaSuccess) A.graph_key = key;
+    return e;
+}
+
 // Enqueues the whole transport loop of a started run (adr_run_setup with no
 // pause) without waiting (ev[2] / ev[3] bracket it), as flow_loop_async.
 int prt::adr_loop_async(prt_ctx* ctx) {
@@ -710,9 +743,7 @@ int prt::adr_loop_async(prt_ctx* ctx) {
     cudaStream_t s = ctx->stream;
     CK(cudaEventRecord(ctx->ev[2], s));
     if (A.rp.limit > 0) {
-        CK(build_while_graph(s, A.graph, [&](cudaGraphConditionalHandle h, int use) {
-            return adr_emit(ctx, h, use);
-        }));
+        CK(adr_graph(ctx));
         const long long chunks =
             A.graph.conditional ? 1 : (A.rp.limit + A.rp.check - 1) / A.rp.check;
         for (long long r = 0; r < chunks; ++r) CK(cudaGraphLaunch(A.graph.exec, s));
@@ -745,7 +776,7 @@ extern "C" int prt_adr_run(prt_ctx* ctx, const prt_adr_run_params* rp, prt_progr
     CK(cudaMemcpyAsync(&cur, dctrl, sizeof(cur), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     bool use_graph = !graphs_disabled();
-    if (use_graph && !cur.done) CK(build_while_graph(s, A.graph, emit));
+    if (use_graph && !cur.done) CK(adr_graph(ctx));
     CK(cudaEventRecord(ctx->ev[2], s));
     while (!cur.done) {
         if (!use_graph) {

@@ -116,6 +116,9 @@ struct AdrState {
     std::vector<int> slot_of_index;     // ladder index -> slot
     int nslots = 0;
     GraphHolder graph;
+    // what the loop graph bakes in (adr_graph_key): a run whose key equals
+    // the cached graph's replays it instead of capturing a new one
+    std::vector<unsigned char> graph_key;
     // Ends the transport state.  Device buffers of at most keep_bytes stay
     // with the context for its next run (every run sizes them with ensure()
     // and initialises what it reads), so back-to-back solves on one context
@@ -125,10 +128,19 @@ struct AdrState {
                          &ladder, &slot_of_step, &idx, &cnt, &total, &tree_leaf_start,
                          &tree_leaf_len, &tree_inner_l, &tree_inner_r, &tree_level_off, &tree_vals,
                          &means, &src_slot, &ctrl, &log, &tmp, &vstats};
+        bool freed = false;
         for (DevBuf* b : all)
-            if (b->bytes > keep_bytes) b->release();
+            if (b->bytes > keep_bytes) {
+                freed = freed || b->p != nullptr;
+                b->release();
+            }
         staged = false;
-        graph.release();
+        // the cached loop graph holds device pointers: it goes with any
+        // buffer that is freed (a kept run's next key compares them anyway)
+        if (freed || keep_bytes == 0) {
+            graph.release();
+            graph_key.clear();
+        }
         keep_steps.clear();
         slot_of_index.clear();
         begun = ran = false;

@@ -130,3 +130,39 @@ def test_transport_with_and_without_programmatic_launch(monkeypatch, pdl):
         assert np.array_equal(tn, z["t_norm"]), name
         assert np.array_equal(prog, z["progress"]), name
         assert np.array_equal(out, z["out"]), (name, float(np.abs(out - z["out"]).max()))
+
+
+def test_cached_loop_graph_follows_every_change():
+    """A transport solve replays the previous solve's loop graph when nothing
+    the graph holds has changed.  Alternating solves on one context that
+    differ in grid, chemistry, Peclet number, step count and chemicals --
+    A, B, C, A, B, C, then A again after a PRT_PDL flip -- each match their
+    golden runs bit for bit."""
+    import os
+    from prtlb_gpu import _lib, solve_adr
+    names = ["adr_spheres3d_monod", "adr_spheres3d_ns4", "adr_disks2d_first"]
+    ctx = _lib.Context(0)
+    try:
+        for rep in range(2):
+            for name in names:
+                z = load_golden(name)
+                with contextlib.redirect_stdout(io.StringIO()):
+                    out, tn = solve_adr(z["mat"], z["vel"], ctx=ctx, **adr_kwargs(z, name))
+                assert np.array_equal(out, z["out"]) and np.array_equal(tn, z["t_norm"]), name
+        z = load_golden(names[0])
+        kw = adr_kwargs(z, names[0])
+        for pdl in ("0", "1"):
+            os.environ["PRT_PDL"] = pdl
+            try:
+                with contextlib.redirect_stdout(io.StringIO()):
+                    out, tn = solve_adr(z["mat"], z["vel"], ctx=ctx, **kw)
+            finally:
+                os.environ.pop("PRT_PDL", None)
+            assert np.array_equal(out, z["out"])
+        kw2 = dict(kw, steps=kw["steps"] // 2)
+        with contextlib.redirect_stdout(io.StringIO()):
+            half, _ = solve_adr(z["mat"], z["vel"], ctx=ctx, **kw2)
+            full, _ = solve_adr(z["mat"], z["vel"], ctx=ctx, **kw)
+        assert np.array_equal(full, z["out"]) and not np.array_equal(half, full)
+    finally:
+        ctx.close()
