@@ -433,15 +433,20 @@ def run_batched(args, torch):
         lo, hi = 24, 96
         reqs, draws = batched_set(args.requests, seed=SEED)
     gen_s = time.perf_counter() - t
-    small, _ = batched_set(2, seed=SEED + 1, nit=200, max_steps=200)
+    # warm-up: the same solves cut to 200 iterations and steps, so every
+    # kernel variant, graph shape and allocation of the timed runs is met first
+    small, _ = request_set(args.requests, lo, hi, seed=SEED, nit=200, max_steps=200)
     ctx = _lib.Context(0)
-    for _ in range(args.warmup):  # warm-up: libraries, graphs, allocator
+    for _ in range(args.warmup):
         [plain_solve(r, ctx) for r in small]
         solve_batch(small, quiet=True)
+        solve_batch(small, quiet=True, mode="streams")
     torch.cuda.synchronize()
     with Clocks(0) as clk:
         t0 = time.perf_counter()
-        res = solve_batch(reqs, quiet=True, mode="tiles")
+        bstats = {}
+        res = solve_batch(reqs, quiet=True, mode="tiles", graph_steps=args.graph_steps,
+                          stats=bstats)
         torch.cuda.synchronize()
         t_batch = time.perf_counter() - t0
         t0 = time.perf_counter()
@@ -471,11 +476,15 @@ def run_batched(args, torch):
                                        n, lo, hi),
                        "voxels": cells, "seed": SEED, "geometry_s": round(gen_s, 2)},
             "mode": "tiles: one persistent launch per class of solves per step over a work "
-                    "list of 256-voxel tiles, K steps per CUDA graph, autotuned tiling",
+                    "list of 256-voxel tiles, %d steps per CUDA graph, autotuned tiling"
+                    % args.graph_steps,
             "plain": {"solves_per_hour": n / t_plain * 3600.0, "seconds": t_plain},
             "streams": {"solves_per_hour": n / t_streams * 3600.0, "seconds": t_streams,
                         "identical_to_plain": all(_same(a, b) for a, b in zip(res_streams, ref))},
             "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": same,
+            "tiling": {"tile_blocks": int(bstats["tile_blocks"]),
+                       "grid_mult": int(bstats["grid_mult"]),
+                       "launches": int(bstats["launches"]), "steps": int(bstats["steps"])},
             "ceiling": ceiling,
             "failed": sum(1 for r in res if r.error is not None), "clocks": clk.summary()}
 
@@ -688,6 +697,8 @@ def main():
                     choices=["plain", "batched", "served", "precision"])
     ap.add_argument("--adr-sweep-steps", type=int, default=3000)
     ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--graph-steps", type=int, default=20,
+                    help="batched mode: batch steps per graph replay between host checks")
     ap.add_argument("--edge-lo", type=int, default=0,
                     help="batched mode: smallest cubic edge (default: the batched set's 24)")
     ap.add_argument("--edge-hi", type=int, default=0,

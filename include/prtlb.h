@@ -305,7 +305,8 @@ int prt_flow_finish(prt_ctx* ctx, float* vel_out, prt_flow_info* info);
 int prt_adr_stage_flow(prt_ctx* ctx, const prt_adr_geom* geom, prt_adr_stats* stats);
 
 /* Frees the flow lattices and maps of ctx (keeps the material grid and the
- * field staged for transport). */
+ * field staged for transport).  A context in a batch may call it once its
+ * flow solve is finished (prt_flow_finish). */
 int prt_flow_release(prt_ctx* ctx);
 
 /* Sets up the transport run of prt_adr_run (after prt_adr_begin) without

@@ -484,10 +484,16 @@ __device__ inline float leaf_sum(const float* __restrict__ s, const int* __restr
 
 // The inner levels of the tree for one species (the whole block takes
 // part), then mean = (0 + sum) / nm in float32 as ndarray.mean() does.
+// L2: the node values are read through L2 (other blocks of the launch wrote
+// the leaves).
+template <bool L2 = false>
 __device__ inline void tree_mean(const PairTree& t, long long nm, float* v, float* mean) {
     for (int h = 0; h < t.nlevel; ++h) {
-        for (int i = t.level_off[h] + threadIdx.x; i < t.level_off[h + 1]; i += blockDim.x)
-            v[t.nleaf + i] = v[t.inner_l[i]] + v[t.inner_r[i]];
+        for (int i = t.level_off[h] + threadIdx.x; i < t.level_off[h + 1]; i += blockDim.x) {
+            const float* a = v + t.inner_l[i];
+            const float* b = v + t.inner_r[i];
+            v[t.nleaf + i] = L2 ? __ldcg(a) + __ldcg(b) : *a + *b;
+        }
         __syncthreads();
     }
     if (threadIdx.x == 0) {

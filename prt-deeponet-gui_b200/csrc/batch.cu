@@ -9,12 +9,15 @@
 // flow_ctrl_advance, so a job's iterations, decisions and final field are
 // bit-identical to the single-solve loop whatever else shares the batch.
 //
-// The control block of a job advances once all its blocks are done: every
-// tile adds its block count to the job's arrival counter, and the tile that
-// completes the count sums the partials (when the iteration samples the
-// convergence mean), advances the control block and clears the counter.
-// Tiles of the same job read the control block before they arrive, so the
-// update cannot race with them.
+// A job's iteration count is implicit: the batch counts its steps on the
+// device, and a job that joined when the batch had done s0 steps with c0
+// iterations behind it is at c0 + (steps done) - s0 = (steps done) - g0.
+// So the control block is written only when the iteration samples the
+// convergence mean or reaches the cap: then every tile adds its block count
+// to the job's arrival counter, and the tile that completes the count sums
+// the partials, advances the control block (flow_ctrl_advance) and clears
+// the counter.  Tiles of the same job read the control block before they
+// arrive, so the update cannot race with them.
 #include "lb_core.cuh"
 
 namespace prt {
@@ -22,7 +25,8 @@ namespace prt {
 template <class L, class M>
 __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
     batch_flow_kernel(const FlowJob* __restrict__ jobs, const BatchTile* __restrict__ tiles,
-                      const int* __restrict__ ntiles_p) {
+                      const int* __restrict__ ntiles_p, const long long* __restrict__ gstep,
+                      int k) {
     using S = typename M::S;
     __shared__ int s_last;
     __shared__ __align__(16) FlowJob sj;  // the tile's job: constants read where they are used
@@ -34,6 +38,7 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
     int t0, t1, cur = -1;
     tile_range(*ntiles_p, t0, t1);
     bool waited = false;
+    long long done_steps = 0;  // batch steps done before this one
     for (int t = t0; t < t1; ++t) {
         const BatchTile tl = tiles[t];
         if (tl.job != cur) {  // uniform over the block
@@ -44,11 +49,14 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
         if (!waited) {  // uniform over the block
             griddep_wait();
             waited = true;
+            done_steps = __ldcg(gstep) + k;
         }
         FlowCtrl* ctrl = sj.ctrl;
-        const long long it = __ldcg(&ctrl->it_base);
-        const bool run = !__ldcg(&ctrl->done) && it < __ldcg(&ctrl->nit);
+        const long long it = done_steps - sj.g0;  // iterations done before this one
+        const long long nit = __ldcg(&ctrl->nit);
+        const bool run = !__ldcg(&ctrl->done) && it < nit;
         const bool check = ((it + 1) % __ldcg(&ctrl->every)) == 0;  // the sampled iterations
+        const bool advance = check || it + 1 >= nit;
         if (!run) {  // uniform over the block
             __syncthreads();  // every thread has read ctrl before sj may change
             continue;
@@ -57,10 +65,14 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
         const Lat<S> lat = lattices<L>(static_cast<S*>(sj.f), nf, (it & 1) != 0);
 #pragma unroll 1
         for (int b = tl.b0; b < tl.b0 + tl.nb; ++b) {
-            const int k = b * kFlowThreads + threadIdx.x;
+            const int slot = b * kFlowThreads + threadIdx.x;
             double acc = 0.0;
-            if (k < nf) acc = lb_cell_rw<L, M>(lat, sj.fm, sj.g, sj.kc, k);
+            if (slot < nf) acc = lb_cell_rw<L, M>(lat, sj.fm, sj.g, sj.kc, slot);
             if (check) block_sum_store(acc, sj.partials + b);
+        }
+        if (!advance) {  // uniform over the block
+            __syncthreads();  // every thread is done with sj before it may change
+            continue;
         }
         // every warp has read the control block and finished its voxels
         // before the tile arrives (the last arrival advances the block)
@@ -86,7 +98,7 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
 
 template <class L, class M>
 static cudaError_t launch_batch_t(const FlowJob* jobs, const BatchTile* tiles, const int* ntiles,
-                                  int grid, cudaStream_t s) {
+                                  const long long* gstep, int k, int grid, cudaStream_t s) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kFlowThreads);
@@ -96,7 +108,7 @@ static cudaError_t launch_batch_t(const FlowJob* jobs, const BatchTile* tiles, c
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, batch_flow_kernel<L, M>, jobs, tiles, ntiles);
+    return cudaLaunchKernelEx(&cfg, batch_flow_kernel<L, M>, jobs, tiles, ntiles, gstep, k);
 }
 
 template <class L, class M>
@@ -123,8 +135,16 @@ static int occupancy_t() {
     return FN<D2Q9, ModeF16>(__VA_ARGS__);
 
 cudaError_t batch_launch_flow(int nd, int precision, const FlowJob* jobs, const BatchTile* tiles,
-                              const int* ntiles, int grid, cudaStream_t s) {
-    PRT_BATCH_DISPATCH(launch_batch_t, jobs, tiles, ntiles, grid, s)
+                              const int* ntiles, const long long* gstep, int k, int grid,
+                              cudaStream_t s) {
+    PRT_BATCH_DISPATCH(launch_batch_t, jobs, tiles, ntiles, gstep, k, grid, s)
+}
+
+__global__ void batch_gstep_kernel(long long* gstep, int k) { *gstep += k; }
+
+cudaError_t batch_launch_gstep(long long* gstep, int k, cudaStream_t s) {
+    batch_gstep_kernel<<<1, 1, 0, s>>>(gstep, k);
+    return cudaGetLastError();
 }
 
 int batch_flow_occupancy(int nd, int precision) { PRT_BATCH_DISPATCH(occupancy_t) }

@@ -6,12 +6,15 @@
 // loop.  Every batch step advances each of them by one iteration (flow) or
 // one step (transport): one persistent launch per class of jobs -- (lattice,
 // precision) for flow, (dimension, species) for transport -- walks a work
-// list of voxel tiles of all jobs of the class.  Flow and transport
-// chains are captured on two streams, so they overlap in the graph.  Work
+// list of voxel tiles of all jobs of the class.  Each class's chain of
+// launches is captured on its own stream, so the classes overlap in the
+// graph.  Work
 // lists, job descriptors and counts live in device memory and the launches
 // read their lengths there, so a graph stays valid while jobs come and go;
 // it is rebuilt only when the set of classes, a grid size or a buffer
 // address changes.
+#include <cmath>
+#include <cstdlib>
 #include <mutex>
 #include <new>
 
@@ -24,9 +27,7 @@ namespace {
 constexpr int kFlowClasses = 8;  // (nd 2|3) x 4 precisions
 constexpr int kAdrClasses = 16;  // (nd 2|3) x species 1..8
 constexpr int kClasses = kFlowClasses + kAdrClasses;
-constexpr int kCountLeaf = kClasses;      // counts[]: tiles per class, leaf items,
-constexpr int kCountAdrJobs = kClasses + 1;  // transport jobs
-constexpr int kCounts = kClasses + 2;
+constexpr int kCounts = kClasses;  // counts[]: tiles per class
 
 int flow_class(int nd, int precision) { return (nd == 3 ? 4 : 0) + precision; }
 int adr_class(int nd, int ns) { return kFlowClasses + (nd == 3 ? 8 : 0) + (ns - 1); }
@@ -49,6 +50,16 @@ struct Candidate {
 // grid_mult 0: one block per work-list entry (no persistent loop)
 const Candidate kCandidates[] = {{1, 0}, {1, 1}, {2, 1}, {4, 0}};
 constexpr int kNumCandidates = 4;
+// launches timed per candidate; its cost is the cheapest of them (the first
+// launch after a rebuild also uploads the new graph)
+constexpr int kTunePasses = 2;
+// the candidates are timed again when the flow solves' share of the work
+// has moved this far from the share they were timed on (the best tiling of
+// a batch of flow solves is not that of a batch of transport runs), or the
+// work itself has grown or shrunk by this factor (few blocks want one block
+// per tile, many want longer tiles)
+constexpr double kRetuneShift = 0.3;
+constexpr double kRetuneScale = 1.5;
 
 }  // namespace
 
@@ -56,8 +67,12 @@ struct prt_batch {
     int device = 0;
     int nsm = 148;
     int K = 20;  // steps per graph replay
-    cudaStream_t stream = nullptr, side = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr, t0 = nullptr, t1 = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+    // one stream per class while a graph is captured: the classes' chains
+    // are independent (no job is in two classes), so they run side by side
+    cudaStream_t cls_stream[kClasses] = {};
+    cudaEvent_t cls_join[kClasses] = {};
     std::string err;
     std::mutex mu;
     std::vector<prt_ctx*> jobs;  // in the batch
@@ -67,12 +82,12 @@ struct prt_batch {
     int nflow = 0, nadr = 0;
     std::vector<FlowJob> h_flow;
     std::vector<AdrJob> h_adr;
-    std::vector<LeafItem> h_leaf;
     std::vector<const int*> h_done;
     std::vector<BatchTile> h_tiles[kClasses];
     int h_counts[kCounts] = {};
-    int grid[kClasses + 2] = {};  // per class, leaf, ctrl
-    GrowBuf d_flow, d_adr, d_leaf, d_done, d_status, d_arrive, d_counts;
+    int grid[kClasses] = {};
+    GrowBuf d_flow, d_adr, d_done, d_status, d_arrive, d_adr_cnt, d_counts;
+    GrowBuf d_gstep;  // batch steps done (one long long), advanced by each replay
     GrowBuf d_tiles[kClasses];
     int* h_status = nullptr;  // pinned
     size_t h_status_cap = 0;
@@ -81,9 +96,11 @@ struct prt_batch {
     std::vector<long long> graph_key;
     // tiling
     int tile_blocks = 1, grid_mult = 1;
-    bool tuning = true;
-    int cand = 0;
+    bool auto_tile = true, tuning = true;
+    int cand = 0, cand_pass = 0;
     double cand_cost[kNumCandidates] = {};
+    double tune_share = -1.0;  // flow share of the work the tiling was timed on
+    long long tune_blocks = 0;  // and its blocks
     // the launch in flight
     bool in_flight = false;
     int launch_replays = 0;
@@ -114,12 +131,33 @@ int bcuda(prt_batch* b, cudaError_t e, const char* what) {
 
 bool is_flow_job(const prt_ctx* c) { return c->flow_armed; }
 
+// The flow solves' share of the batch's blocks of work, and their number.
+double flow_share(const prt_batch* b, long long* blocks = nullptr) {
+    long long fl = 0, all = 0;
+    for (const prt_ctx* c : b->jobs) {
+        const long long n = is_flow_job(c) ? c->flow.nb : c->adr.nbk;
+        all += n;
+        if (is_flow_job(c)) fl += n;
+    }
+    if (blocks) *blocks = all;
+    return all ? (double)fl / (double)all : 0.0;
+}
+
+// The g0 of a job (see FlowJob): fixed at the first launch after it joined,
+// from the batch steps done then and the count it joined with.
+long long job_g0(prt_batch* b, prt_ctx* c) {
+    if (!c->batch_g0_set) {
+        c->batch_g0 = b->steps_run - c->batch_c0;
+        c->batch_g0_set = true;
+    }
+    return c->batch_g0;
+}
+
 // Job lists, work lists and grids for the current jobs; uploads them.
 int rebuild(prt_batch* b) {
     b->order.clear();
     b->h_flow.clear();
     b->h_adr.clear();
-    b->h_leaf.clear();
     b->h_done.clear();
     for (int c = 0; c < kClasses; ++c) b->h_tiles[c].clear();
     for (prt_ctx* c : b->jobs)
@@ -130,6 +168,7 @@ int rebuild(prt_batch* b) {
     b->nadr = (int)b->order.size() - b->nflow;
     const int T = b->tile_blocks;
     long long blocks = 0;
+    size_t adr_cnt = 0;  // transport counters: per job, arrival + seams
     for (int i = 0; i < b->nflow; ++i) {
         prt_ctx* c = b->order[i];
         FlowState& F = c->flow;
@@ -142,6 +181,7 @@ int rebuild(prt_batch* b) {
         J.partials = F.partials.as<double>();
         J.arrive = nullptr;  // set after the counter array is sized
         J.nb = F.nb;
+        J.g0 = job_g0(b, c);
         b->h_flow.push_back(J);
         const int cls = flow_class(F.p.nd, F.p.precision);
         for (int b0 = 0; b0 < F.nb; b0 += T)
@@ -157,23 +197,55 @@ int rebuild(prt_batch* b) {
         J.p = A.p;
         J.ctrl = A.ctrl.as<AdrCtrl>();
         J.means = A.means.as<float>();
+        J.cnt = nullptr;  // set after the counter array is sized
+        J.blk_leaf = A.blk_leaf.as<const int>();
+        J.nbk = A.nbk;
+        J.g0 = job_g0(b, c);
         b->h_adr.push_back(J);
         const int cls = adr_class(A.d.nd, A.d.ns);
-        const int nbk = (int)((A.d.nm + 255) / 256);
+        const int nbk = A.nbk;
         for (int b0 = 0; b0 < nbk; b0 += T)
             b->h_tiles[cls].push_back(BatchTile{i, b0, std::min(T, nbk - b0), 0});
+        // a run without solute voxels still steps (its control block
+        // advances) through one empty tile
+        if (nbk == 0) b->h_tiles[cls].push_back(BatchTile{i, 0, 0, 0});
         blocks += nbk;
-        for (int sp = 0; sp < A.d.ns; ++sp)
-            for (int l0 = 0; l0 < A.d.tree.nleaf; l0 += 256)
-                b->h_leaf.push_back(LeafItem{i, sp, l0, 0});
+        adr_cnt += (size_t)nbk + 1;
         b->h_done.push_back(&J.ctrl->done);
+    }
+    // pull tables: each solve chose them against the whole L2 cache; in a
+    // batch they pay only while the flow jobs' lattices and tables together
+    // fit in half of it, otherwise the tables' bytes add to the DRAM traffic
+    // and the kernels look the upstream slots up through the maps (the same
+    // slots either way, so the fields do not change)
+    {
+        long long ws = 0, l2 = 0;
+        for (int i = 0; i < b->nflow; ++i) {
+            const prt_ctx* c = b->order[i];
+            const FlowState& F = c->flow;
+            const int q = F.p.nd == 3 ? 19 : 9;
+            const long long es = F.p.precision == PRT_FP64 ? 8 : F.p.precision == PRT_FP16 ? 2 : 4;
+            ws += 2ll * q * F.fm.nf * es + (F.fm.nbr ? flow_nbr_bytes(q, F.fm.nf) / 2 : 0);
+            l2 = c->l2_bytes;
+        }
+        const char* v = std::getenv("PRT_NBR_TABLE");
+        const bool forced = v && v[0] == '1';
+        if (!forced && ws > l2 / 2)
+            for (FlowJob& J : b->h_flow) J.fm.nbr = nullptr;
     }
     const int njobs = (int)b->order.size();
     BK(b->d_arrive.fit((size_t)std::max(b->nflow, 1) * sizeof(unsigned)));
     for (int i = 0; i < b->nflow; ++i) b->h_flow[i].arrive = b->d_arrive.b.as<unsigned>() + i;
+    BK(b->d_adr_cnt.fit(std::max<size_t>(adr_cnt, 1) * sizeof(unsigned)));
+    {
+        unsigned* at = b->d_adr_cnt.b.as<unsigned>();
+        for (AdrJob& J : b->h_adr) {
+            J.cnt = at;
+            at += J.nbk + 1;
+        }
+    }
     BK(b->d_flow.fit(std::max<size_t>(b->h_flow.size(), 1) * sizeof(FlowJob)));
     BK(b->d_adr.fit(std::max<size_t>(b->h_adr.size(), 1) * sizeof(AdrJob)));
-    BK(b->d_leaf.fit(std::max<size_t>(b->h_leaf.size(), 1) * sizeof(LeafItem)));
     BK(b->d_done.fit((size_t)std::max(njobs, 1) * sizeof(int*)));
     BK(b->d_status.fit((size_t)std::max(njobs, 1) * sizeof(int)));
     BK(b->d_counts.fit(kCounts * sizeof(int)));
@@ -192,22 +264,18 @@ int rebuild(prt_batch* b) {
             BK(cudaMemcpyAsync(b->d_tiles[c].b.p, b->h_tiles[c].data(),
                                b->h_tiles[c].size() * sizeof(BatchTile), cudaMemcpyHostToDevice, s));
     }
-    b->h_counts[kCountLeaf] = (int)b->h_leaf.size();
-    b->h_counts[kCountAdrJobs] = b->nadr;
     if (!b->h_flow.empty())
         BK(cudaMemcpyAsync(b->d_flow.b.p, b->h_flow.data(), b->h_flow.size() * sizeof(FlowJob),
                            cudaMemcpyHostToDevice, s));
     if (!b->h_adr.empty())
         BK(cudaMemcpyAsync(b->d_adr.b.p, b->h_adr.data(), b->h_adr.size() * sizeof(AdrJob),
                            cudaMemcpyHostToDevice, s));
-    if (!b->h_leaf.empty())
-        BK(cudaMemcpyAsync(b->d_leaf.b.p, b->h_leaf.data(), b->h_leaf.size() * sizeof(LeafItem),
-                           cudaMemcpyHostToDevice, s));
     if (njobs)
         BK(cudaMemcpyAsync(b->d_done.b.p, b->h_done.data(), (size_t)njobs * sizeof(int*),
                            cudaMemcpyHostToDevice, s));
     BK(cudaMemcpyAsync(b->d_counts.b.p, b->h_counts, sizeof(b->h_counts), cudaMemcpyHostToDevice, s));
     BK(cudaMemsetAsync(b->d_arrive.b.p, 0, (size_t)std::max(b->nflow, 1) * sizeof(unsigned), s));
+    BK(cudaMemsetAsync(b->d_adr_cnt.b.p, 0, std::max<size_t>(adr_cnt, 1) * sizeof(unsigned), s));
     // the host vectors must outlive the copies
     BK(cudaStreamSynchronize(s));
     // persistent grids: grid_mult resident waves, at most one block per tile
@@ -223,8 +291,6 @@ int rebuild(prt_batch* b) {
         b->grid[c] = b->grid_mult == 0 ? nt
                                        : std::max(1, std::min(nt, b->grid_mult * occ * b->nsm));
     }
-    b->grid[kClasses] = std::max(1, std::min((int)b->h_leaf.size(), 4 * b->nsm));
-    b->grid[kClasses + 1] = std::max(1, std::min(b->nadr, 2 * b->nsm));
     b->launch_blocks = blocks;
     b->last_tiles = 0;
     for (int c = 0; c < kClasses; ++c) b->last_tiles += b->h_counts[c];
@@ -232,63 +298,64 @@ int rebuild(prt_batch* b) {
     return PRT_OK;
 }
 
-// One batch step, flow launches on s_flow and transport launches on s_adr.
-cudaError_t emit_step(prt_batch* b, cudaStream_t s_flow, cudaStream_t s_adr) {
+// One batch step: the launch of class c on streams[c], or on `s` for every
+// class when streams is null.
+cudaError_t emit_step(prt_batch* b, cudaStream_t s, const cudaStream_t* streams, int k) {
     const int* counts = b->d_counts.b.as<int>();
-    for (int c = 0; c < kFlowClasses; ++c) {
+    for (int c = 0; c < kClasses; ++c) {
         if (!b->grid[c]) continue;
-        cudaError_t e = batch_launch_flow(c >= 4 ? 3 : 2, c % 4, b->d_flow.b.as<FlowJob>(),
-                                          b->d_tiles[c].b.as<BatchTile>(), counts + c, b->grid[c],
-                                          s_flow);
+        cudaStream_t sc = streams ? streams[c] : s;
+        cudaError_t e;
+        if (c < kFlowClasses) {
+            e = batch_launch_flow(c >= 4 ? 3 : 2, c % 4, b->d_flow.b.as<FlowJob>(),
+                                  b->d_tiles[c].b.as<BatchTile>(), counts + c,
+                                  b->d_gstep.b.as<long long>(), k, b->grid[c], sc);
+        } else {
+            const int a = c - kFlowClasses;
+            e = batch_launch_adr(a >= 8 ? 3 : 2, a % 8 + 1, b->d_adr.b.as<AdrJob>(),
+                                 b->d_tiles[c].b.as<BatchTile>(), counts + c,
+                                 b->d_gstep.b.as<long long>(), k, b->grid[c], sc);
+        }
         if (e != cudaSuccess) return e;
     }
-    if (b->nadr == 0) return cudaSuccess;
-    for (int c = kFlowClasses; c < kClasses; ++c) {
-        if (!b->grid[c]) continue;
-        const int k = c - kFlowClasses;
-        cudaError_t e = batch_launch_adr(k >= 8 ? 3 : 2, k % 8 + 1, b->d_adr.b.as<AdrJob>(),
-                                         b->d_tiles[c].b.as<BatchTile>(), counts + c, b->grid[c],
-                                         s_adr);
-        if (e != cudaSuccess) return e;
-    }
-    cudaError_t e = cudaSuccess;
-    if (!b->h_leaf.empty())
-        e = batch_launch_adr_leaf(b->d_adr.b.as<AdrJob>(), b->d_leaf.b.as<LeafItem>(),
-                                  counts + kCountLeaf, b->grid[kClasses], s_adr);
-    if (e != cudaSuccess) return e;
-    return batch_launch_adr_ctrl(b->d_adr.b.as<AdrJob>(), counts + kCountAdrJobs,
-                                 b->grid[kClasses + 1], s_adr);
+    return cudaSuccess;
 }
 
 int launches_per_step(const prt_batch* b) {
     int n = 0;
     for (int c = 0; c < kClasses; ++c) n += b->grid[c] ? 1 : 0;
-    if (b->nadr) n += 1 + (b->h_leaf.empty() ? 0 : 1);
     return n;
 }
 
-// Graph of K steps: the flow chain on the batch stream, the transport
-// chain on the side stream, joined at the end.
+// Graph of K steps: each class's chain of K launches on its own stream,
+// forked from and joined back to the batch stream.
 int ensure_graph(prt_batch* b) {
     std::vector<long long> key;
     key.push_back(b->K);
-    key.push_back(b->nadr > 0);
-    key.push_back(!b->h_leaf.empty());
-    for (int c = 0; c < kClasses + 2; ++c) key.push_back(b->grid[c]);
+    for (int c = 0; c < kClasses; ++c) key.push_back(b->grid[c]);
     key.push_back((long long)b->d_flow.b.p);
     key.push_back((long long)b->d_adr.b.p);
-    key.push_back((long long)b->d_leaf.b.p);
     key.push_back((long long)b->d_counts.b.p);
     for (int c = 0; c < kClasses; ++c) key.push_back((long long)b->d_tiles[c].b.p);
     if (b->graph.exec && key == b->graph_key) return PRT_OK;
     b->graph.release();
+    for (int c = 0; c < kClasses; ++c) {
+        if (!b->grid[c] || b->cls_stream[c]) continue;
+        BK(cudaStreamCreateWithFlags(&b->cls_stream[c], cudaStreamNonBlocking));
+        BK(cudaEventCreateWithFlags(&b->cls_join[c], cudaEventDisableTiming));
+    }
     cudaStream_t s = b->stream;
     BK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaEventRecord(b->fork, s);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->fork, 0);
-    for (int k = 0; k < b->K && e == cudaSuccess; ++k) e = emit_step(b, s, b->side);
-    if (e == cudaSuccess) e = cudaEventRecord(b->join, b->side);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->join, 0);
+    for (int c = 0; c < kClasses && e == cudaSuccess; ++c)
+        if (b->grid[c]) e = cudaStreamWaitEvent(b->cls_stream[c], b->fork, 0);
+    for (int k = 0; k < b->K && e == cudaSuccess; ++k) e = emit_step(b, s, b->cls_stream, k);
+    for (int c = 0; c < kClasses && e == cudaSuccess; ++c) {
+        if (!b->grid[c]) continue;
+        e = cudaEventRecord(b->cls_join[c], b->cls_stream[c]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->cls_join[c], 0);
+    }
+    if (e == cudaSuccess) e = batch_launch_gstep(b->d_gstep.b.as<long long>(), b->K, s);
     cudaGraph_t g = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(s, &g);
     if (e != cudaSuccess) {
@@ -315,6 +382,7 @@ void prt::batch_detach(prt_ctx* c) {
         if (o == c) o = nullptr;
     b->dirty = true;
     c->batch = nullptr;
+    c->batch_g0_set = false;
 }
 
 // ===========================================================================
@@ -383,7 +451,10 @@ extern "C" int prt_adr_stage_flow(prt_ctx* ctx, const prt_adr_geom* geom, prt_ad
 
 extern "C" int prt_flow_release(prt_ctx* ctx) {
     if (!ctx) return PRT_E_INVALID;
-    if (ctx->batch) return fail(ctx, PRT_E_STATE, "the context is in a batch");
+    // a context in a batch may drop its lattices once its flow solve is
+    // finished: the batch's kernels no longer touch them
+    if (ctx->batch && ctx->flow_armed)
+        return fail(ctx, PRT_E_STATE, "the context's flow solve is in a batch");
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->flow.release_lattices();
@@ -493,11 +564,12 @@ extern "C" int prt_batch_create(int device, int32_t graph_steps, prt_batch** out
     e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreate(&b->t0);
     if (e == cudaSuccess) e = cudaEventCreate(&b->t1);
+    if (e == cudaSuccess) e = b->d_gstep.fit(sizeof(long long));
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_gstep.b.p, 0, sizeof(long long), b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) {
         set_noctx_error(cudaGetErrorString(e));
         prt_batch_destroy(b);
@@ -517,15 +589,18 @@ extern "C" void prt_batch_destroy(prt_batch* b) {
         b->jobs.clear();
     }
     b->graph.release();
-    GrowBuf* all[] = {&b->d_flow, &b->d_adr, &b->d_leaf, &b->d_done, &b->d_status, &b->d_arrive,
-                      &b->d_counts};
+    GrowBuf* all[] = {&b->d_flow, &b->d_adr, &b->d_done, &b->d_status, &b->d_arrive,
+                      &b->d_adr_cnt, &b->d_counts, &b->d_gstep};
     for (GrowBuf* g : all) g->b.release();
     for (int c = 0; c < kClasses; ++c) b->d_tiles[c].b.release();
     if (b->h_status) cudaFreeHost(b->h_status);
-    cudaEvent_t evs[] = {b->fork, b->join, b->t0, b->t1};
+    cudaEvent_t evs[] = {b->fork, b->t0, b->t1};
     for (cudaEvent_t ev : evs)
         if (ev) cudaEventDestroy(ev);
-    if (b->side) cudaStreamDestroy(b->side);
+    for (int c = 0; c < kClasses; ++c) {
+        if (b->cls_join[c]) cudaEventDestroy(b->cls_join[c]);
+        if (b->cls_stream[c]) cudaStreamDestroy(b->cls_stream[c]);
+    }
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -539,9 +614,21 @@ extern "C" int prt_batch_add(prt_batch* b, prt_ctx* job) {
     if (!job->flow_armed && !job->adr_armed)
         return bfail(b, PRT_E_STATE, "the context has no started flow solve or transport run");
     if (job->running) return bfail(b, PRT_E_STATE, "the context's loop is running on its stream");
+    // the count the job joins with (the batch advances it implicitly)
+    BK(cudaSetDevice(job->device));
+    long long c0 = 0;
+    if (job->flow_armed)
+        BK(cudaMemcpyAsync(&c0, &job->flow.ctrl.as<FlowCtrl>()->it_base, sizeof(c0),
+                           cudaMemcpyDeviceToHost, job->stream));
+    else
+        BK(cudaMemcpyAsync(&c0, &job->adr.ctrl.as<AdrCtrl>()->n_base, sizeof(c0),
+                           cudaMemcpyDeviceToHost, job->stream));
+    BK(cudaStreamSynchronize(job->stream));
     std::lock_guard<std::mutex> lk(b->mu);
     b->jobs.push_back(job);
     job->batch = b;
+    job->batch_c0 = c0;
+    job->batch_g0_set = false;
     b->dirty = true;
     return PRT_OK;
 }
@@ -550,6 +637,33 @@ extern "C" int prt_batch_remove(prt_batch* b, prt_ctx* job) {
     if (!b || !job) return bfail(b, PRT_E_INVALID, "null argument");
     if (job->batch != b) return bfail(b, PRT_E_INVALID, "the context is not in this batch");
     if (b->in_flight) return bfail(b, PRT_E_STATE, "wait for the launch before removing jobs");
+    // a job leaving before its loop ended gets its count written back: the
+    // batch writes it to the control block only on the steps that check
+    if (job->batch_g0_set) {
+        BK(cudaSetDevice(b->device));
+        const long long count = b->steps_run - job->batch_g0;
+        cudaStream_t s = job->stream;
+        if (job->flow_armed) {
+            FlowCtrl fc;
+            BK(cudaMemcpyAsync(&fc, job->flow.ctrl.p, sizeof(fc), cudaMemcpyDeviceToHost, s));
+            BK(cudaStreamSynchronize(s));
+            if (!fc.done) {
+                fc.it_base = count;
+                fc.iters = count;
+                BK(cudaMemcpyAsync(job->flow.ctrl.p, &fc, sizeof(fc), cudaMemcpyHostToDevice, s));
+                BK(cudaStreamSynchronize(s));
+            }
+        } else {
+            AdrCtrl ac;
+            BK(cudaMemcpyAsync(&ac, job->adr.ctrl.p, sizeof(ac), cudaMemcpyDeviceToHost, s));
+            BK(cudaStreamSynchronize(s));
+            if (!ac.done) {
+                ac.n_base = count;
+                BK(cudaMemcpyAsync(job->adr.ctrl.p, &ac, sizeof(ac), cudaMemcpyHostToDevice, s));
+                BK(cudaStreamSynchronize(s));
+            }
+        }
+    }
     batch_detach(job);
     return PRT_OK;
 }
@@ -560,6 +674,19 @@ extern "C" int prt_batch_launch(prt_batch* b, int32_t steps) {
     if (b->in_flight) return bfail(b, PRT_E_STATE, "the previous launch was not waited for");
     BK(cudaSetDevice(b->device));
     std::lock_guard<std::mutex> lk(b->mu);
+    if (b->dirty && b->auto_tile && !b->tuning && !b->jobs.empty()) {
+        long long blocks = 0;
+        const double share = flow_share(b, &blocks);
+        if (std::fabs(share - b->tune_share) > kRetuneShift ||
+            (double)blocks * kRetuneScale < (double)b->tune_blocks ||
+            (double)blocks > kRetuneScale * (double)b->tune_blocks) {
+            b->tuning = true;
+            b->cand = 0;
+            b->cand_pass = 0;
+        }
+    }
+    if (b->tuning && b->cand == 0 && b->cand_pass == 0)
+        b->tune_share = flow_share(b, &b->tune_blocks);
     if (b->tuning) {
         const Candidate& cd = kCandidates[b->cand];
         if (cd.tile_blocks != b->tile_blocks || cd.grid_mult != b->grid_mult) {
@@ -583,15 +710,18 @@ extern "C" int prt_batch_launch(prt_batch* b, int32_t steps) {
     BK(cudaEventRecord(b->t0, s));
     if (njobs > 0 && replays > 0) {
         if (!use_graph) {
-            for (int r = 0; r < replays * b->K; ++r) {
-                // without a graph both chains go on the batch stream
-                cudaError_t e = emit_step(b, s, s);
-                if (e != cudaSuccess) return bcuda(b, e, "batch step launch");
+            for (int r = 0; r < replays; ++r) {
+                // without a graph every class goes on the batch stream
+                for (int k = 0; k < b->K; ++k) {
+                    cudaError_t e = emit_step(b, s, nullptr, k);
+                    if (e != cudaSuccess) return bcuda(b, e, "batch step launch");
+                }
+                BK(batch_launch_gstep(b->d_gstep.b.as<long long>(), b->K, s));
             }
         } else {
             for (int r = 0; r < replays; ++r) BK(cudaGraphLaunch(b->graph.exec, s));
         }
-        b->launches += (int64_t)replays * b->K * launches_per_step(b);
+        b->launches += (int64_t)replays * (b->K * launches_per_step(b) + 1);
     }
     if (njobs > 0) {
         BK(batch_launch_status(b->d_done.b.as<const int* const>(), njobs, b->d_status.b.as<int>(), s));
@@ -625,8 +755,12 @@ extern "C" int prt_batch_wait(prt_batch* b, int32_t* n_done) {
     if (n_done) *n_done = done;
     // tiling choice: cost per block-step of each candidate, then the cheapest
     if (b->tuning && b->launch_replays > 0 && b->launch_blocks > 0) {
-        b->cand_cost[b->cand] = ms / ((double)b->launch_replays * b->K * (double)b->launch_blocks);
-        b->cand += 1;
+        const double cost = ms / ((double)b->launch_replays * b->K * (double)b->launch_blocks);
+        if (b->cand_pass == 0 || cost < b->cand_cost[b->cand]) b->cand_cost[b->cand] = cost;
+        if (++b->cand_pass == kTunePasses) {
+            b->cand_pass = 0;
+            b->cand += 1;
+        }
         if (b->cand == kNumCandidates) {
             int best = 0;
             for (int i = 1; i < kNumCandidates; ++i)
@@ -685,14 +819,17 @@ extern "C" int prt_batch_tune(prt_batch* b, int32_t tile_blocks, int32_t grid_mu
     if (!b) return PRT_E_INVALID;
     std::lock_guard<std::mutex> lk(b->mu);
     if (tile_blocks == 0) {
+        b->auto_tile = true;
         b->tuning = true;
         b->cand = 0;
+        b->cand_pass = 0;
         return PRT_OK;
     }
     if (!(tile_blocks == 1 || tile_blocks == 2 || tile_blocks == 4) ||
         !(grid_mult == 0 || grid_mult == 1 || grid_mult == 2))
         return bfail(b, PRT_E_INVALID,
                      "tile blocks must be 1, 2 or 4 and the grid multiple 0, 1 or 2");
+    b->auto_tile = false;
     b->tuning = false;
     if (tile_blocks != b->tile_blocks || grid_mult != b->grid_mult) b->dirty = true;
     b->tile_blocks = tile_blocks;
@@ -709,7 +846,7 @@ extern "C" int prt_batch_stats(const prt_batch* b, double* out8) {
     out8[4] = (double)b->steps_run;
     out8[5] = b->last_ms;
     out8[6] = (double)b->last_tiles;
-    out8[7] = 0;
+    out8[7] = b->tuning ? 1.0 : 0.0;
     return PRT_OK;
 }
 

@@ -313,24 +313,30 @@ struct FlowJob {
     FlowCtrl* ctrl;
     double* partials;  // one per block of slots, as in the single solve
     unsigned* arrive;
+    long long g0;      // the job has run (batch steps done) - g0 iterations
     int nb;            // blocks of slots of the job
     int pad;
 };
 
-// One transport solve of a batch.
+// Solute voxels per block of a batched transport job.
+constexpr int kBatchAdrBlock = 256;
+
+// One transport solve of a batch.  Its solute voxels are cut into nbk blocks
+// of kBatchAdrBlock.  On a check step each block sums the pairwise-tree
+// leaves that lie inside it; a leaf that crosses the seam between blocks
+// b - 1 and b is summed by whichever of the two finishes second (counter
+// cnt[1 + b]), and the block that completes the job's arrival count
+// (cnt[0]) forms the means, applies the stop rule and advances the control
+// block.  The counters are back at zero after every step.
 struct AdrJob {
     AdrDev d;
     prt_adr_params p;
     AdrCtrl* ctrl;
-    float* means;  // ns floats: the pore means of the latest check
-};
-
-// A leaf work-list entry: leaves [leaf0, leaf0 + 256) of species `species`
-// of transport job `job`.
-struct LeafItem {
-    int job;
-    int species;
-    int leaf0;
+    float* means;          // ns floats: the pore means of the latest check
+    unsigned* cnt;         // arrival counter, then one counter per seam (nbk + 1)
+    const int* blk_leaf;   // nbk + 1 entries: first leaf starting in block b
+    long long g0;          // the job has run (batch steps done) - g0 steps
+    int nbk;
     int pad;
 };
 
@@ -355,15 +361,20 @@ __device__ __forceinline__ void tile_range(int n, int& t0, int& t1) {
 // Each launch is persistent: `grid` blocks walk the work list, whose length
 // is read on the device so a captured graph stays valid when the list is
 // rewritten between replays.
+// The step kernels take the batch's step counter (steps completed before
+// the current graph replay) and their step's place k in the replay; a job's
+// own count is that plus k minus its g0, so its control block is written
+// only on the steps that sample, check or end it.
 cudaError_t batch_launch_flow(int nd, int precision, const FlowJob* jobs, const BatchTile* tiles,
-                              const int* ntiles, int grid, cudaStream_t s);
+                              const int* ntiles, const long long* gstep, int k, int grid,
+                              cudaStream_t s);
 int batch_flow_occupancy(int nd, int precision);
 cudaError_t batch_launch_adr(int nd, int ns, const AdrJob* jobs, const BatchTile* tiles,
-                             const int* ntiles, int grid, cudaStream_t s);
+                             const int* ntiles, const long long* gstep, int k, int grid,
+                             cudaStream_t s);
+// *gstep += k: ends a graph replay of k batch steps.
+cudaError_t batch_launch_gstep(long long* gstep, int k, cudaStream_t s);
 int batch_adr_occupancy(int nd, int ns);
-cudaError_t batch_launch_adr_leaf(const AdrJob* jobs, const LeafItem* items, const int* nitems,
-                                  int grid, cudaStream_t s);
-cudaError_t batch_launch_adr_ctrl(const AdrJob* jobs, const int* njobs, int grid, cudaStream_t s);
 cudaError_t batch_launch_status(const int* const* done_ptrs, int n, int* out, cudaStream_t s);
 
 }  // namespace prt

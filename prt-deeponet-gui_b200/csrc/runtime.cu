@@ -487,6 +487,19 @@ extern "C" int prt_adr_stage_dev(prt_ctx* ctx, const uint8_t* d_mat, const float
         CK(cudaMemcpyAsync(A.tree_inner_r.p, ir.data(), (size_t)I * 4, cudaMemcpyHostToDevice, s));
     }
     CK(cudaMemcpyAsync(A.tree_level_off.p, loff.data(), (size_t)(nlevel + 1) * 4, cudaMemcpyHostToDevice, s));
+    // the first leaf of each block of the batch engine (leaves start in order)
+    A.nbk = (int)((nm + kBatchAdrBlock - 1) / kBatchAdrBlock);
+    std::vector<int> bl((size_t)A.nbk + 1);
+    {
+        int leaf = 0;
+        for (int b = 0; b <= A.nbk; ++b) {
+            const long long at = (long long)b * kBatchAdrBlock;
+            while (leaf < L && tb.leaf_start[leaf] < at) ++leaf;
+            bl[b] = leaf;
+        }
+    }
+    CK(A.blk_leaf.ensure(bl.size() * 4));
+    CK(cudaMemcpyAsync(A.blk_leaf.p, bl.data(), bl.size() * 4, cudaMemcpyHostToDevice, s));
     A.d.tree.nleaf = L;
     A.d.tree.ninner = I;
     A.d.tree.nlevel = nlevel;

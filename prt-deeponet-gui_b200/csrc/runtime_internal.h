@@ -105,6 +105,10 @@ struct AdrState {
     DevBuf mat, vel, flags, mflag, face[3], buf[2], ladder, slot_of_step, idx, cnt, total;
     DevBuf tree_leaf_start, tree_leaf_len, tree_inner_l, tree_inner_r, tree_level_off, tree_vals;
     DevBuf means, src_slot, ctrl, log;
+    // for the batch engine: blk_leaf[b] = the first leaf starting at or after
+    // solute voxel kBatchAdrBlock * b (b = 0 .. nbk), see AdrJob
+    DevBuf blk_leaf;
+    int nbk = 0;
     bool staged = false;
     prt_adr_geom geom{};
     const uint8_t* d_mat = nullptr;  // staged inputs (borrowed until begin)
@@ -127,7 +131,7 @@ struct AdrState {
         DevBuf* all[] = {&mat, &vel, &flags, &mflag, &face[0], &face[1], &face[2], &buf[0], &buf[1],
                          &ladder, &slot_of_step, &idx, &cnt, &total, &tree_leaf_start,
                          &tree_leaf_len, &tree_inner_l, &tree_inner_r, &tree_level_off, &tree_vals,
-                         &means, &src_slot, &ctrl, &log, &tmp, &vstats};
+                         &means, &src_slot, &ctrl, &log, &tmp, &vstats, &blk_leaf};
         bool freed = false;
         for (DevBuf* b : all)
             if (b->bytes > keep_bytes) {
@@ -175,6 +179,9 @@ struct prt_ctx {
     bool flow_armed = false;  // flow set up, its time loop not finished
     bool adr_armed = false;   // transport run set up, its time loop not finished
     prt_batch* batch = nullptr;  // the batch holding this context, if any
+    long long batch_c0 = 0;      // iterations / steps done when it joined the batch
+    long long batch_g0 = 0;      // its count is (batch steps done) - batch_g0
+    bool batch_g0_set = false;   // batch_g0 is fixed at the first launch after joining
     int running = 0;             // a loop enqueued by prt_*_launch: 1 flow, 2 transport
     long long l2_bytes = 0;      // the device's L2 cache
 };

@@ -418,9 +418,9 @@ def _run(ctx, S, n_t, steps, tol, max_steps, info, ratio, da, da_abio, on_progre
     return outputs(ctx, S, n_t, n, ks, picked, steps, max_steps, info, da, da_abio)
 
 
-def outputs(ctx, S, n_t, n, ks, picked, steps, max_steps, info, da, da_abio):
+def outputs(ctx, S, n_t, n, ks, picked, steps, max_steps, info, da, da_abio, end=True):
     """(out, t_norm) and the info keys of a finished run (prtlb_3d.py:1565-1595);
-    ends the transport state of the context."""
+    ends the transport state of the context unless `end` is false."""
     L = _lib.lib()
     total = int(max(n, 1))
     repeated = n_t - len(set(picked))
@@ -432,7 +432,8 @@ def outputs(ctx, S, n_t, n, ks, picked, steps, max_steps, info, da, da_abio):
             ctx.check(L.prt_adr_fetch(ctx.handle, int(i), buf.ctypes.data_as(ctypes.c_void_p)))
             cache[i] = buf
         out[j] = cache[i]
-    L.prt_adr_end(ctx.handle)
+    if end:
+        L.prt_adr_end(ctx.handle)
     t_norm = (ks[picked].astype(np.float32) / total).astype(np.float32)
     hit_cap = steps is None and n >= max_steps
     if info is not None:

@@ -115,6 +115,7 @@ class Batch(object):
         self._jobs = {}
         self._ready = []      # collected solves waiting for their host work
         self._graveyard = []  # finished contexts, freed when the device is idle
+        self._unlattice = []  # contexts past their flow loop: lattices freed then too
         self._in_flight = False
         self.finished = []
 
@@ -146,11 +147,12 @@ class Batch(object):
 
     def stats(self):
         """Kernel launches, graph builds, tile blocks, grid multiple, steps
-        run, last launch ms, tiles of the last launch."""
+        run, last launch ms, tiles of the last launch, and 1 while the
+        tiling candidates are still being timed."""
         out = (ctypes.c_double * 8)()
         self._check(_lib.lib().prt_batch_stats(self.handle, out))
         keys = ("launches", "graph_builds", "tile_blocks", "grid_mult", "steps", "last_ms",
-                "tiles")
+                "tiles", "tuning")
         return {k: float(out[i]) for i, k in enumerate(keys)}
 
     def tune(self, tile_blocks=0, grid_mult=0):
@@ -246,6 +248,11 @@ class Batch(object):
         return done
 
     def _bury(self):
+        L = _lib.lib()
+        for ctx in self._unlattice:
+            if ctx.handle:
+                ctx.check(L.prt_flow_release(ctx.handle))
+        self._unlattice = []
         for ctx in self._graveyard:
             ctx.close()
         self._graveyard = []
@@ -256,12 +263,18 @@ class Batch(object):
         return self.wait()
 
     def run(self, max_steps=None):
-        """Advance until every solve has finished (or `max_steps` steps)."""
+        """Advance until every solve has finished (or `max_steps` steps).
+        The host work of the solves collected by one wait (a finished flow
+        solve's field and transport set-up, a finished run's snapshots) is
+        done while the next graph replay runs, as in the served loop."""
         out = []
         n = 0
         while self._jobs and (max_steps is None or n < max_steps):
-            out.extend(self.advance())
+            self.launch()
+            out.extend(self.process())
+            self.wait(process=False)
             n += self.graph_steps
+        out.extend(self.process())
         return out
 
     # -- phase changes ----------------------------------------------------
@@ -305,7 +318,9 @@ class Batch(object):
                              mat=req.mat)
         job.S = S
         ctx.check(L.prt_adr_begin(ctx.handle, ctypes.byref(S.params)))
-        ctx.check(L.prt_flow_release(ctx.handle))
+        # the lattices are freed once the device is idle (a free now would
+        # wait for the launch in flight)
+        self._unlattice.append(ctx)
         R = _adr.run_params(S, a["steps"], a["tol"], a["max_steps"], a["ratio"])
         ctx.check(L.prt_adr_start(ctx.handle, ctypes.byref(R)))
         self._enqueue(ctx, "adr")
@@ -322,14 +337,15 @@ class Batch(object):
         picked = _adr.pick(ks, n, int(a["n_t"]))
         res.steps = n
         res.adr_info = {}
+        # the context is destroyed once the device is idle, which frees the
+        # transport state (ending it here would wait for the launch in flight)
         if req.fetch:
             res.out, res.t_norm = _adr.outputs(ctx, S, int(a["n_t"]), n, ks, picked, a["steps"],
                                                a["max_steps"], res.adr_info, a["da"],
-                                               a["da_abio"])
+                                               a["da_abio"], end=False)
         else:
             total = int(max(n, 1))
             res.t_norm = (ks[picked].astype(np.float32) / total).astype(np.float32)
-            L.prt_adr_end(ctx.handle)
         job.phase = "done"
 
 
@@ -350,6 +366,7 @@ class StreamBatch(Batch):
         self._jobs = {}
         self._ready = []
         self._graveyard = []
+        self._unlattice = []
         self._in_flight = False
         self.finished = []
         self._launches = 0
@@ -415,15 +432,18 @@ def _needs_host_stage(req):
     return chem is not None and getattr(chem, "biofilm_code", None) is not None
 
 
-def solve_batch(requests, device=0, graph_steps=20, quiet=False, mode="tiles"):
+def solve_batch(requests, device=0, graph_steps=20, quiet=False, mode="tiles", stats=None):
     """Solve every Request in one batch; Results in request order.  mode
     "tiles": the batch engine's persistent tile-list kernels; "streams":
-    concurrent single-solve loops (StreamBatch)."""
+    concurrent single-solve loops (StreamBatch).  A dict given as `stats`
+    receives the batch's final statistics."""
     b = (StreamBatch(device=device, quiet=quiet) if mode == "streams"
          else Batch(device=device, graph_steps=graph_steps, quiet=quiet))
     try:
         results = [b.submit(r) for r in requests]
         b.run()
+        if stats is not None:
+            stats.update(b.stats())
         return results
     finally:
         b.close()
