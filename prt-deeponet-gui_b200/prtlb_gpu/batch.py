@@ -16,9 +16,11 @@ the velocity field staying on the device) and finished transport runs to
 their ``Result``.
 """
 
+import atexit
 import contextlib
 import ctypes
 import io
+import threading
 import time
 
 import numpy as np
@@ -31,6 +33,51 @@ FLOW_DEFAULTS = dict(nit=30000, force=2e-6, tau_lb=0.8, magic=3.0 / 16.0, tol=1e
                      precision="fp64")
 ADR_DEFAULTS = dict(n_species=2, steps=None, tol=2e-3, max_steps=100000, ratio=1.12, chem=None,
                     da_abio=0.0)
+
+
+# Idle contexts kept for the next solves on a device (at most _POOL_CAP):
+# a solve that takes one reuses its device buffers instead of allocating
+# them, and a finished solve's context costs no cudaFree.  What a kept
+# context holds: the material grid and velocity field of its last solve and
+# the transport buffers up to the keep size of prt_adr_end (256 MiB each).
+_POOL_CAP = 64
+_pool = {}
+_pool_lock = threading.Lock()
+
+
+def _take_context(device):
+    with _pool_lock:
+        kept = _pool.get(device)
+        if kept:
+            return kept.pop()
+    return _lib.Context(device)
+
+
+def _return_context(ctx, device):
+    """A finished solve's context, with the device idle: kept, or closed
+    when it failed or the pool is full."""
+    if not ctx.handle:
+        return
+    if not getattr(ctx, "broken", False):
+        _lib.lib().prt_adr_end(ctx.handle)  # frees transport buffers above the keep size
+        with _pool_lock:
+            kept = _pool.setdefault(device, [])
+            if len(kept) < _POOL_CAP:
+                kept.append(ctx)
+                return
+    ctx.close()
+
+
+def release_contexts():
+    """Close the idle contexts kept for reuse (and free their memory)."""
+    with _pool_lock:
+        kept = [c for lst in _pool.values() for c in lst]
+        _pool.clear()
+    for c in kept:
+        c.close()
+
+
+atexit.register(release_contexts)
 
 
 class Request(object):
@@ -177,7 +224,7 @@ class Batch(object):
         f = req.flow
         g, p = _flow.flow_params(req.mat, nd, name, f["nit"], f["force"], f["tau_lb"],
                                  f["magic"], f["tol"], f["precision"])
-        ctx = _lib.Context(self.device)
+        ctx = _take_context(self.device)
         try:
             L = _lib.lib()
             ctx.check(L.prt_flow_start(ctx.handle, g.ctypes.data_as(ctypes.c_void_p),
@@ -237,6 +284,7 @@ class Batch(object):
             except (Exception, SystemExit) as e:  # SystemExit: a dead flow
                 job.res.error = e
                 job.phase = "done"
+                job.ctx.broken = True  # closed, not kept for another solve
             if job.phase == "done":
                 job.res.t_done = time.perf_counter()
                 del self._jobs[job.ctx.handle.value]
@@ -254,7 +302,7 @@ class Batch(object):
                 ctx.check(L.prt_flow_release(ctx.handle))
         self._unlattice = []
         for ctx in self._graveyard:
-            ctx.close()
+            _return_context(ctx, self.device)
         self._graveyard = []
 
     def advance(self, steps=None):
@@ -266,14 +314,25 @@ class Batch(object):
         """Advance until every solve has finished (or `max_steps` steps).
         The host work of the solves collected by one wait (a finished flow
         solve's field and transport set-up, a finished run's snapshots) is
-        done while the next graph replay runs, as in the served loop."""
+        done while the next graph replay runs, as in the served loop.
+        Between solves that finish, one launch runs up to 8 graph replays
+        (doubling while no solve finished), so the host's per-launch work
+        is paid less often; a solve that finishes is then seen at most 8
+        replays late, while the other solves keep advancing."""
         out = []
         n = 0
+        reps = 1
         while self._jobs and (max_steps is None or n < max_steps):
-            self.launch()
+            steps = self.graph_steps * reps
+            if max_steps is not None:
+                steps = min(steps, max_steps - n)
+            self.launch(steps)
+            quiet = not self._ready
             out.extend(self.process())
             self.wait(process=False)
-            n += self.graph_steps
+            quiet = quiet and not self._ready
+            reps = min(reps * 2, 8) if quiet else 1
+            n += steps
         out.extend(self.process())
         return out
 
