@@ -22,11 +22,20 @@
 
 namespace prt {
 
-template <class L, class M>
+// UNI: every job of the launch has the constants `kcu` (the same force, tau
+// and magic number), which the kernel then reads as a parameter, like the
+// single-solve step, instead of from the job's descriptor in shared memory.
+template <bool UNI>
+__device__ __forceinline__ const LbParams& job_constants(const LbParams& kcu, const LbParams& own) {
+    if constexpr (UNI) return kcu;
+    else return own;
+}
+
+template <class L, class M, bool UNI>
 __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
     batch_flow_kernel(const FlowJob* __restrict__ jobs, const BatchTile* __restrict__ tiles,
                       const int* __restrict__ ntiles_p, const long long* __restrict__ gstep,
-                      int k) {
+                      int k, LbParams kcu) {
     using S = typename M::S;
     __shared__ int s_last;
     __shared__ __align__(16) FlowJob sj;  // the tile's job: constants read where they are used
@@ -67,7 +76,8 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
         for (int b = tl.b0; b < tl.b0 + tl.nb; ++b) {
             const int slot = b * kFlowThreads + threadIdx.x;
             double acc = 0.0;
-            if (slot < nf) acc = lb_cell_rw<L, M>(lat, sj.fm, sj.g, sj.kc, slot);
+            if (slot < nf)
+                acc = lb_cell_rw<L, M>(lat, sj.fm, sj.g, job_constants<UNI>(kcu, sj.kc), slot);
             if (check) block_sum_store(acc, sj.partials + b);
         }
         if (!advance) {  // uniform over the block
@@ -98,7 +108,8 @@ __global__ void __launch_bounds__(kFlowThreads, M::batch_min_blocks)
 
 template <class L, class M>
 static cudaError_t launch_batch_t(const FlowJob* jobs, const BatchTile* tiles, const int* ntiles,
-                                  const long long* gstep, int k, int grid, cudaStream_t s) {
+                                  const long long* gstep, int k, const LbParams* uniform,
+                                  int grid, cudaStream_t s) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kFlowThreads);
@@ -108,14 +119,18 @@ static cudaError_t launch_batch_t(const FlowJob* jobs, const BatchTile* tiles, c
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, batch_flow_kernel<L, M>, jobs, tiles, ntiles, gstep, k);
+    if (uniform)
+        return cudaLaunchKernelEx(&cfg, batch_flow_kernel<L, M, true>, jobs, tiles, ntiles, gstep,
+                                  k, *uniform);
+    return cudaLaunchKernelEx(&cfg, batch_flow_kernel<L, M, false>, jobs, tiles, ntiles, gstep, k,
+                              LbParams{});
 }
 
 template <class L, class M>
 static int occupancy_t() {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_flow_kernel<L, M>, kFlowThreads,
-                                                      0) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_flow_kernel<L, M, false>,
+                                                      kFlowThreads, 0) != cudaSuccess) {
         cudaGetLastError();
         return 1;
     }
@@ -135,9 +150,9 @@ static int occupancy_t() {
     return FN<D2Q9, ModeF16>(__VA_ARGS__);
 
 cudaError_t batch_launch_flow(int nd, int precision, const FlowJob* jobs, const BatchTile* tiles,
-                              const int* ntiles, const long long* gstep, int k, int grid,
-                              cudaStream_t s) {
-    PRT_BATCH_DISPATCH(launch_batch_t, jobs, tiles, ntiles, gstep, k, grid, s)
+                              const int* ntiles, const long long* gstep, int k,
+                              const LbParams* uniform, int grid, cudaStream_t s) {
+    PRT_BATCH_DISPATCH(launch_batch_t, jobs, tiles, ntiles, gstep, k, uniform, grid, s)
 }
 
 __global__ void batch_gstep_kernel(long long* gstep, int k) { *gstep += k; }

@@ -15,6 +15,7 @@
 // address changes.
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <mutex>
 #include <new>
 
@@ -86,6 +87,9 @@ struct prt_batch {
     std::vector<BatchTile> h_tiles[kClasses];
     int h_counts[kCounts] = {};
     int grid[kClasses] = {};
+    // flow classes whose jobs all share their constants (passed as a parameter)
+    bool flow_uni[kFlowClasses] = {};
+    LbParams flow_kc[kFlowClasses] = {};
     GrowBuf d_flow, d_adr, d_done, d_status, d_arrive, d_adr_cnt, d_counts;
     GrowBuf d_gstep;  // batch steps done (one long long), advanced by each replay
     GrowBuf d_tiles[kClasses];
@@ -233,6 +237,21 @@ int rebuild(prt_batch* b) {
         if (!forced && ws > l2 / 2)
             for (FlowJob& J : b->h_flow) J.fm.nbr = nullptr;
     }
+    for (int c = 0; c < kFlowClasses; ++c) b->flow_uni[c] = false;
+    {
+        bool seen[kFlowClasses] = {}, differ[kFlowClasses] = {};
+        for (int i = 0; i < b->nflow; ++i) {
+            const FlowState& F = b->order[i]->flow;
+            const int c = flow_class(F.p.nd, F.p.precision);
+            if (!seen[c]) {
+                seen[c] = true;
+                b->flow_kc[c] = b->h_flow[i].kc;
+            } else if (std::memcmp(&b->flow_kc[c], &b->h_flow[i].kc, sizeof(LbParams)) != 0) {
+                differ[c] = true;
+            }
+        }
+        for (int c = 0; c < kFlowClasses; ++c) b->flow_uni[c] = seen[c] && !differ[c];
+    }
     const int njobs = (int)b->order.size();
     BK(b->d_arrive.fit((size_t)std::max(b->nflow, 1) * sizeof(unsigned)));
     for (int i = 0; i < b->nflow; ++i) b->h_flow[i].arrive = b->d_arrive.b.as<unsigned>() + i;
@@ -309,7 +328,8 @@ cudaError_t emit_step(prt_batch* b, cudaStream_t s, const cudaStream_t* streams,
         if (c < kFlowClasses) {
             e = batch_launch_flow(c >= 4 ? 3 : 2, c % 4, b->d_flow.b.as<FlowJob>(),
                                   b->d_tiles[c].b.as<BatchTile>(), counts + c,
-                                  b->d_gstep.b.as<long long>(), k, b->grid[c], sc);
+                                  b->d_gstep.b.as<long long>(), k,
+                                  b->flow_uni[c] ? &b->flow_kc[c] : nullptr, b->grid[c], sc);
         } else {
             const int a = c - kFlowClasses;
             e = batch_launch_adr(a >= 8 ? 3 : 2, a % 8 + 1, b->d_adr.b.as<AdrJob>(),
@@ -333,6 +353,13 @@ int ensure_graph(prt_batch* b) {
     std::vector<long long> key;
     key.push_back(b->K);
     for (int c = 0; c < kClasses; ++c) key.push_back(b->grid[c]);
+    for (int c = 0; c < kFlowClasses; ++c) {  // constants baked into the launches
+        key.push_back(b->flow_uni[c]);
+        if (!b->flow_uni[c]) continue;
+        long long w[(sizeof(LbParams) + 7) / 8] = {};
+        std::memcpy(w, &b->flow_kc[c], sizeof(LbParams));
+        for (long long x : w) key.push_back(x);
+    }
     key.push_back((long long)b->d_flow.b.p);
     key.push_back((long long)b->d_adr.b.p);
     key.push_back((long long)b->d_counts.b.p);

@@ -365,9 +365,10 @@ __device__ __forceinline__ void tile_range(int n, int& t0, int& t1) {
 // the current graph replay) and their step's place k in the replay; a job's
 // own count is that plus k minus its g0, so its control block is written
 // only on the steps that sample, check or end it.
+// uniform: the constants every job of the launch shares, or null.
 cudaError_t batch_launch_flow(int nd, int precision, const FlowJob* jobs, const BatchTile* tiles,
-                              const int* ntiles, const long long* gstep, int k, int grid,
-                              cudaStream_t s);
+                              const int* ntiles, const long long* gstep, int k,
+                              const LbParams* uniform, int grid, cudaStream_t s);
 int batch_flow_occupancy(int nd, int precision);
 cudaError_t batch_launch_adr(int nd, int ns, const AdrJob* jobs, const BatchTile* tiles,
                              const int* ntiles, const long long* gstep, int k, int grid,

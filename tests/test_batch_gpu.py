@@ -38,8 +38,10 @@ def _requests():
                      flow=dict(nit=550, tol=1e-6, precision="fp64"),
                      adr=dict(pe=3.0, da=0.3, n_t=3, n_species=1, chem=first_order_chemistry(),
                               steps=420), tag="first3"))
+    # the same class as monod3 with other constants: its flow launches read
+    # them per job instead of as one shared parameter
     R.append(Request(_pack3((24, 10, 12), 0.55, 3),
-                     flow=dict(nit=800, tol=0.0, precision="fp32"),
+                     flow=dict(nit=800, tol=0.0, precision="fp32", tau_lb=0.9),
                      adr=dict(pe=30.0, da=2.0, n_t=5, n_species=2,
                               chem=reversible_sorption_chemistry(0.5, 2.0), max_steps=1800),
                      tag="sorb3"))
