@@ -418,6 +418,32 @@ def _same(res, ref):
     return bool(np.array_equal(res.out, ref[0]) and np.array_equal(res.t_norm, ref[1]))
 
 
+def profile_batched(args, torch):
+    """A short batch for kernel profiles: the batched set's solves capped at
+    --profile-nit flow iterations and --profile-steps transport steps, one
+    fixed tiling, the batch alone (no plain or concurrent arms), graphs as
+    PRT_GRAPHS says.  Prints what ran; it is not a measurement."""
+    from prtlb_gpu.batch import Batch
+    from prtlb_gpu.workloads import request_set
+    lo, hi = args.edge_lo or 24, args.edge_hi or 96
+    reqs, _ = request_set(args.requests, lo, hi, seed=SEED, nit=args.profile_nit,
+                          max_steps=args.profile_steps)
+    tb, gm = (int(x) for x in args.profile_tiling.split(","))
+    b = Batch(device=0, graph_steps=args.graph_steps, quiet=True)
+    try:
+        b.tune(tb, gm)
+        res = [b.submit(r) for r in reqs]
+        b.run()
+        st = b.stats()
+    finally:
+        b.close()
+    torch.cuda.synchronize()
+    return {"profile": "batched", "requests": len(reqs), "edges": [lo, hi],
+            "flow_nit": args.profile_nit, "transport_steps": args.profile_steps,
+            "tiling": [tb, gm], "failed": sum(r.error is not None for r in res),
+            "launches": int(st["launches"]), "steps": int(st["steps"])}
+
+
 def run_batched(args, torch):
     """48 uneven geometries (edges 24-96): the batch engine against the same
     solves one at a time."""
@@ -697,6 +723,13 @@ def main():
                     choices=["plain", "batched", "served", "precision"])
     ap.add_argument("--adr-sweep-steps", type=int, default=3000)
     ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--profile-nit", type=int, default=0,
+                    help="batched mode: a short batch for kernel profiles, solves capped at "
+                         "this many flow iterations")
+    ap.add_argument("--profile-steps", type=int, default=600,
+                    help="with --profile-nit: transport steps per solve")
+    ap.add_argument("--profile-tiling", default="4,0",
+                    help="with --profile-nit: tile blocks, grid multiple")
     ap.add_argument("--graph-steps", type=int, default=20,
                     help="batched mode: batch steps per graph replay between host checks")
     ap.add_argument("--edge-lo", type=int, default=0,
@@ -710,6 +743,8 @@ def main():
     if args.mode != "plain" and args.impl == "ours":
         import torch
         fn = {"batched": run_batched, "served": run_served, "precision": run_precision}[args.mode]
+        if args.mode == "batched" and args.profile_nit:
+            fn = profile_batched
         print(json.dumps(fn(args, torch)))
         return
     globals().update(EDGE=args.edge, FLOW_NIT=args.flow_nit, ADR_STEPS=args.adr_steps)

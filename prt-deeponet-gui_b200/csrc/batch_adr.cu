@@ -22,6 +22,10 @@ namespace prt {
 namespace {
 constexpr int kBatchAdrThreads = kBatchAdrBlock;
 constexpr int kWarps = kBatchAdrThreads / 32;
+// four resident blocks (64 registers): measured against 5, 6 and 8, which
+// spill in the voxel step (32.1 against 33.8, 35.1 and 41.8 us a step for
+// 48 small transport runs); without a bound the step takes 80-95 registers
+constexpr int kBatchAdrMinBlocks = 4;
 }
 
 // leaf_sum of one leaf (at most 128 values) by one warp, with the same float
@@ -61,8 +65,11 @@ __device__ __forceinline__ float warp_leaf_sum(const float* __restrict__ s,
 // inside it, plus each leaf across one of its two seams when the block is
 // the second of the two blocks to get there.  Every thread of the block
 // calls it.
+// Not inlined, like job_step_end: the rare check-step code keeps its
+// registers to itself, so the voxel step runs at the occupancy of its own
+// register needs.
 template <int NS>
-__device__ void block_leaves(const AdrJob& J, int b, long long n, float (*sh)[128]) {
+__device__ __noinline__ void block_leaves(const AdrJob& J, int b, long long n, float (*sh)[128]) {
     __shared__ int s_lo, s_hi, s_l0, s_l1;
     const PairTree& tr = J.d.tree;
     if (threadIdx.x == 0) {
@@ -115,8 +122,31 @@ __device__ void block_leaves(const AdrJob& J, int b, long long n, float (*sh)[12
     __syncthreads();  // s_* are reused by the block's next call
 }
 
+// The end of step n of job J by the block that completed its arrival count
+// (every thread of the block calls it): on a check step the tree levels, the
+// means and the stop rule; then the step count, the end at the limit, and
+// the arrival counter cleared.
+template <int NS>
+__device__ __noinline__ void job_step_end(const AdrJob& J, long long n, long long limit, bool due) {
+    __threadfence();
+    AdrCtrl* ctrl = J.ctrl;
+    if (due) {
+        const PairTree& tr = J.d.tree;
+        for (int sp = 0; sp < NS; ++sp)
+            tree_mean<true>(tr, J.d.nm, J.d.tree_vals + (long long)sp * (tr.nleaf + tr.ninner),
+                            J.means + sp);
+    }
+    if (threadIdx.x == 0) {
+        if (due) adr_check(ctrl, J.means, n, J.d.log, J.d.log_cap);
+        ctrl->n_base = n;
+        if (n >= limit) ctrl->done = 1;
+        J.cnt[0] = 0u;
+        __threadfence();
+    }
+}
+
 template <int ND, int NS>
-__global__ void __launch_bounds__(kBatchAdrThreads)
+__global__ void __launch_bounds__(kBatchAdrThreads, kBatchAdrMinBlocks)
     batch_adr_kernel(const AdrJob* __restrict__ jobs, const BatchTile* __restrict__ tiles,
                      const int* __restrict__ ntiles_p, const long long* __restrict__ gstep, int k) {
     // the tile's job in shared memory: the per-voxel code reads its many
@@ -182,23 +212,7 @@ __global__ void __launch_bounds__(kBatchAdrThreads)
             s_last = (old + (unsigned)tl.nb == (unsigned)J.nbk) ? 1 : 0;
         }
         __syncthreads();
-        if (s_last) {  // uniform over the block
-            __threadfence();
-            if (due) {
-                const PairTree& tr = J.d.tree;
-                for (int sp = 0; sp < NS; ++sp)
-                    tree_mean<true>(tr, J.d.nm,
-                                    J.d.tree_vals + (long long)sp * (tr.nleaf + tr.ninner),
-                                    J.means + sp);
-            }
-            if (threadIdx.x == 0) {
-                if (due) adr_check(ctrl, J.means, n, J.d.log, J.d.log_cap);
-                ctrl->n_base = n;
-                if (n >= limit) ctrl->done = 1;
-                J.cnt[0] = 0u;
-                __threadfence();
-            }
-        }
+        if (s_last) job_step_end<NS>(J, n, limit, due);  // uniform over the block
     }
 }
 
