@@ -325,8 +325,26 @@ def run_ours(args, rank, world, torch, dist):
            "ncell": ncell, "nfluid": nfluid, "e2e_ms": e2e_ms, "e2e_split": e2e_split}
     if rank == 0 and not args.no_side:
         res["side"] = side_measurements(ctx, peak, kind)
+        if world == 1:
+            res["side"]["batched_small_mix"] = batched_side(args, torch)
     ctx.close()
     return res
+
+
+def batched_side(args, torch):
+    """The batch engine on 48 small solves (edges 24-48, the batched set's
+    draws) against the same solves one at a time, as `--mode batched
+    --edge-lo 24 --edge-hi 48` measures it (without its concurrent-solve arm)."""
+    ns = argparse.Namespace(**vars(args))
+    ns.edge_lo, ns.edge_hi, ns.requests, ns.warmup, ns.graph_steps = 24, 48, 48, 1, 20
+    d = run_batched(ns, torch, streams=False)
+    return {"metric": d["metric"], "unit": d["unit"], "value": round(d["value"], 1),
+            "plain_solves_per_hour": round(d["plain"]["solves_per_hour"], 1),
+            "speedup_vs_plain": round(d["speedup_vs_plain"], 3),
+            "identical_to_plain": d["identical_to_plain"], "failed": d["failed"],
+            "workload": d["config"]["workload"], "batch_seconds": round(d["ms_per_step"] / 1e3, 3),
+            "plain_seconds": round(d["plain"]["seconds"], 3), "tiling": d["tiling"],
+            "clocks": d["clocks"]}
 
 
 def side_measurements(ctx, peak, kind):
@@ -444,7 +462,7 @@ def profile_batched(args, torch):
             "launches": int(st["launches"]), "steps": int(st["steps"])}
 
 
-def run_batched(args, torch):
+def run_batched(args, torch, streams=True):
     """48 uneven geometries (edges 24-96): the batch engine against the same
     solves one at a time."""
     from prtlb_gpu import _lib
@@ -466,7 +484,8 @@ def run_batched(args, torch):
     for _ in range(args.warmup):
         [plain_solve(r, ctx) for r in small]
         solve_batch(small, quiet=True)
-        solve_batch(small, quiet=True, mode="streams")
+        if streams:
+            solve_batch(small, quiet=True, mode="streams")
     torch.cuda.synchronize()
     with Clocks(0) as clk:
         t0 = time.perf_counter()
@@ -476,7 +495,7 @@ def run_batched(args, torch):
         torch.cuda.synchronize()
         t_batch = time.perf_counter() - t0
         t0 = time.perf_counter()
-        res_streams = solve_batch(reqs, quiet=True, mode="streams")
+        res_streams = solve_batch(reqs, quiet=True, mode="streams") if streams else None
         torch.cuda.synchronize()
         t_streams = time.perf_counter() - t0
         t0 = time.perf_counter()
@@ -505,8 +524,9 @@ def run_batched(args, torch):
                     "list of 256-voxel tiles, %d steps per CUDA graph, autotuned tiling"
                     % args.graph_steps,
             "plain": {"solves_per_hour": n / t_plain * 3600.0, "seconds": t_plain},
-            "streams": {"solves_per_hour": n / t_streams * 3600.0, "seconds": t_streams,
-                        "identical_to_plain": all(_same(a, b) for a, b in zip(res_streams, ref))},
+            "streams": ({"solves_per_hour": n / t_streams * 3600.0, "seconds": t_streams,
+                         "identical_to_plain": all(_same(a, b) for a, b in zip(res_streams, ref))}
+                        if streams else None),
             "speedup_vs_plain": t_plain / t_batch, "identical_to_plain": same,
             "tiling": {"tile_blocks": int(bstats["tile_blocks"]),
                        "grid_mult": int(bstats["grid_mult"]),
