@@ -174,3 +174,44 @@ def test_concurrent_streams_equal_single_solves(singles):
     for r, q, ref in zip(res, reqs, refs):
         _same(r, ref, q)
     assert st["launches"] >= 2 * sum(1 for q in reqs if q.adr is not None)
+
+
+def test_moving_between_batches_keeps_the_counts(singles):
+    """Solves that leave a batch part-way (prt_batch_remove) and finish in
+    another: one in its flow loop, one in its transport loop.  The batch
+    keeps step counts on the device and writes a job's count to its control
+    block only on check steps, so leaving writes the count back; the results
+    must still equal the single solves."""
+    from prtlb_gpu import _lib
+    from prtlb_gpu.batch import Batch
+    reqs, refs = singles
+    moved = [(reqs[0], refs[0]), (reqs[2], refs[2])]
+    L = _lib.lib()
+    a = Batch(graph_steps=7, quiet=True)
+    b = Batch(graph_steps=11, quiet=True)
+    try:
+        res = [a.submit(q) for q, _ in moved]
+        jobs = list(a._jobs.values())
+
+        def move(job):
+            assert L.prt_batch_remove(a.handle, job.ctx.handle) == _lib.PRT_OK
+            del a._jobs[job.ctx.handle.value]
+            b._jobs[job.ctx.handle.value] = job
+            assert L.prt_batch_add(b.handle, job.ctx.handle) == _lib.PRT_OK
+
+        # the first leaves during its flow loop (cap 700 iterations)
+        a.advance(70)
+        assert jobs[0].phase == "flow"
+        move(jobs[0])
+        # the second once its transport loop has run a while
+        while jobs[1].phase == "flow":
+            a.advance()
+        a.advance(30)
+        assert jobs[1].phase == "adr"
+        move(jobs[1])
+        b.run()
+        for r, (q, ref) in zip(res, moved):
+            _same(r, ref, q)
+    finally:
+        a.close()
+        b.close()
