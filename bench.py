@@ -327,8 +327,24 @@ def run_ours(args, rank, world, torch, dist):
         res["side"] = side_measurements(ctx, peak, kind)
         if world == 1:
             res["side"]["batched_small_mix"] = batched_side(args, torch)
+            res["side"]["served_short"] = served_side(args, torch)
     ctx.close()
     return res
+
+
+def served_side(args, torch):
+    """The served loop on a short stream (the first 16 requests of the served
+    set, edges 32-160, Poisson 20 /s, concurrent solves) against the same
+    stream one at a time, as `--mode served --requests 16` measures it."""
+    ns = argparse.Namespace(**vars(args))
+    ns.requests, ns.rate, ns.serve_mode, ns.warmup = 16, 20.0, "streams", 1
+    d = run_served(ns, torch)
+    keep = ("value", "unit", "latency_p50_s", "latency_p99_s", "queue_p50_s", "completed",
+            "failed", "speedup_vs_plain", "identical_to_plain", "clocks")
+    out = {k: d.get(k) for k in keep}
+    out["plain"] = d.get("plain")
+    out["workload"] = d["config"]["workload"]
+    return out
 
 
 def batched_side(args, torch):
