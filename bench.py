@@ -48,6 +48,7 @@ import multiprocessing as mp
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -108,12 +109,15 @@ def peaks():
 
 
 class Clocks(object):
-    """nvidia-smi sampled every 200 ms while the timed region runs."""
+    """nvidia-smi sampled every 200 ms while the timed region runs; the raw
+    samples go to bench_clocks_<pid>.csv in $PRT_CLOCKS_DIR (default: the
+    system's temporary directory)."""
 
     def __init__(self, gpu):
         self.gpu = gpu
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks_%d.csv" % os.getpid())
+        where = os.environ.get("PRT_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(where, "bench_clocks_%d.csv" % os.getpid())
 
     def __enter__(self):
         try:
