@@ -24,11 +24,12 @@ constexpr int kAdrThreads = 128;
 // during a run (the voxel's index, flags, position and face velocities) is
 // read while the previous step drains; the control block and the
 // concentrations only after griddepcontrol.wait.
+// late: the next step is let in after this one's stores (see pdl_late).
 template <int ND, int NS, bool BF>
 __global__ void __launch_bounds__(kAdrThreads) adr_step_kernel(AdrDev d, prt_adr_params p,
                                                                const AdrCtrl* __restrict__ ctrl,
-                                                               int kstep) {
-    griddep_launch_dependents();
+                                                               int kstep, int late) {
+    if (!late) griddep_launch_dependents();
     const long long kk = (long long)blockIdx.x * kAdrThreads + threadIdx.x;
     const bool live = kk < d.nm;
     VoxelSetup s;
@@ -38,6 +39,7 @@ __global__ void __launch_bounds__(kAdrThreads) adr_step_kernel(AdrDev d, prt_adr
     if (ctrl->done || n > ctrl->limit) return;  // uniform over the grid
     if (!live) return;
     adr_voxel_step<ND, NS, BF>(d, p, n, s);
+    if (late) griddep_launch_dependents();
 }
 
 // ---------------------------------------------------------------------------
@@ -257,11 +259,13 @@ static long long resident_blocks(K kern) {
     return (long long)per_sm * sms;
 }
 
-// Steps whose blocks exceed one resident wave go out with programmatic
-// stream serialisation (128^3: 16.2 -> 15.3 us per step, four chemicals
-// 44.5 -> 40.5); a step that fits in one wave launches plainly, because
-// there the next step's blocks, all resident early, slowed the running one
-// (64^3: 4.32 -> 5.56 us).  PRT_PDL=0 launches every step plainly.
+// Steps go out with programmatic stream serialisation.  One whose blocks
+// exceed one resident wave lets the next step launch at its start (128^3:
+// 16.2 -> 15.3 us per step, four chemicals 44.5 -> 40.5); one that fits in
+// one wave only after its stores (pdl_late), because released at the start
+// the next step's blocks, all resident early, slowed the running one (64^3:
+// 4.32 -> 5.56 us) where released at the end they cut the step to 3.66 us.
+// PRT_PDL=0 launches every step plainly.
 template <int ND, int NS>
 static cudaError_t step_t(const AdrDev& d, const prt_adr_params& p, AdrCtrl* ctrl, int k,
                           cudaStream_t s) {
@@ -276,8 +280,9 @@ static cudaError_t step_t(const AdrDev& d, const prt_adr_params& p, AdrCtrl* ctr
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = (pdl_enabled() && nb > resident_blocks(kern)) ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, kern, d, p, ctrl, k);
+    const int late = pdl_late(nb <= resident_blocks(kern)) ? 1 : 0;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, d, p, ctrl, k, late);
 }
 
 template <int ND>

@@ -148,7 +148,8 @@ __device__ __noinline__ void job_step_end(const AdrJob& J, long long n, long lon
 template <int ND, int NS>
 __global__ void __launch_bounds__(kBatchAdrThreads, kBatchAdrMinBlocks)
     batch_adr_kernel(const AdrJob* __restrict__ jobs, const BatchTile* __restrict__ tiles,
-                     const int* __restrict__ ntiles_p, const long long* __restrict__ gstep, int k) {
+                     const int* __restrict__ ntiles_p, const long long* __restrict__ gstep, int k,
+                     int late) {
     // the tile's job in shared memory: the per-voxel code reads its many
     // constants (feeds, diffusivities, rate constants) from there
     __shared__ __align__(16) AdrJob J;
@@ -157,8 +158,9 @@ __global__ void __launch_bounds__(kBatchAdrThreads, kBatchAdrMinBlocks)
     // programmatic dependent launch: the work list and the job descriptors
     // are not written inside the graph, so the first tile's descriptor is
     // copied while the previous step drains; control blocks, counters and
-    // concentrations are touched only after griddepcontrol.wait
-    griddep_launch_dependents();
+    // concentrations are touched only after griddepcontrol.wait; late: the
+    // next step is let in after this one's work (see pdl_late)
+    if (!late) griddep_launch_dependents();
     int t0, t1, cur = -1;
     tile_range(*ntiles_p, t0, t1);
     bool waited = false;
@@ -214,6 +216,18 @@ __global__ void __launch_bounds__(kBatchAdrThreads, kBatchAdrMinBlocks)
         __syncthreads();
         if (s_last) job_step_end<NS>(J, n, limit, due);  // uniform over the block
     }
+    if (late) griddep_launch_dependents();
+}
+
+template <int ND, int NS>
+static int occ_t() {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_adr_kernel<ND, NS>,
+                                                      kBatchAdrThreads, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return nb > 0 ? nb : 1;
 }
 
 template <int ND, int NS>
@@ -228,19 +242,10 @@ static cudaError_t launch_t(const AdrJob* jobs, const BatchTile* tiles, const in
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, batch_adr_kernel<ND, NS>, jobs, tiles, ntiles, gstep, k);
+    const int late = pdl_late(true) ? 1 : 0;  // as the batched flow step (batch.cu)
+    return cudaLaunchKernelEx(&cfg, batch_adr_kernel<ND, NS>, jobs, tiles, ntiles, gstep, k, late);
 }
 
-template <int ND, int NS>
-static int occ_t() {
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_adr_kernel<ND, NS>,
-                                                      kBatchAdrThreads, 0) != cudaSuccess) {
-        cudaGetLastError();
-        return 1;
-    }
-    return nb > 0 ? nb : 1;
-}
 
 #define PRT_NS_DISPATCH(FN, ND, ...)              \
     switch (ns) {                                 \

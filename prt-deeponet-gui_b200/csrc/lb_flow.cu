@@ -28,12 +28,14 @@
 namespace prt {
 
 // One whole LB iteration t: lattice (t & 1) is read, lattice ((t + 1) & 1)
-// written; solid voxels do nothing.
+// written; solid voxels do nothing.  late: the next iteration is let in
+// after this one's stores (see pdl_late).
 template <class L, class M, bool ODD, bool CHECK>
 __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
     lb_step_kernel(typename M::S* __restrict__ f, FlowMap fm, Grid g, LbParams kc,
-                   const FlowCtrl* __restrict__ ctrl, int kstep, double* __restrict__ partials) {
-    griddep_launch_dependents();
+                   const FlowCtrl* __restrict__ ctrl, int kstep, double* __restrict__ partials,
+                   int late) {
+    if (!late) griddep_launch_dependents();
     const int k = blockIdx.x * kFlowThreads + threadIdx.x;
     const Lat<typename M::S> lat = lattices<L>(f, fm.nf, ODD);
     // the pore maps never change during a solve: the pulls (with tables) or
@@ -54,6 +56,7 @@ __global__ void __launch_bounds__(kFlowThreads, M::min_blocks)
         if (CHECK) acc = ux;
     }
     if (CHECK) block_sum_store(acc, partials + blockIdx.x);
+    if (late) griddep_launch_dependents();
 }
 
 // FlowConvergence.done() at the end of a chunk of `every` iterations
@@ -233,7 +236,9 @@ int flow_blocks(long long n) { return (int)((n + kFlowThreads - 1) / kFlowThread
 // upstream slots (the maps do not change during a solve) and waits in
 // griddepcontrol.wait for t's results.  Measured on the B200 with 128-thread
 // blocks: 64^3 float32 4.89 -> 4.82 us per iteration, float16 4.43 -> 4.18,
-// 128^3 float32 41.3 -> 40.6.
+// 128^3 float32 41.3 -> 40.6.  A grid of one resident wave releases the
+// next step only after its stores (pdl_late): 64^3 float32 collision
+// 4.60 -> 4.09 us.
 
 template <class L, class M, bool ODD, bool CHECK>
 static cudaError_t launch_step_one(typename M::S* f, const FlowMap& fm, const Grid& g,
@@ -249,8 +254,20 @@ static cudaError_t launch_step_one(typename M::S* f, const FlowMap& fm, const Gr
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, lb_step_kernel<L, M, ODD, CHECK>, f, fm, g, k, ctrl, kstep,
-                              partials);
+    auto kern = lb_step_kernel<L, M, ODD, CHECK>;
+    static const long long resident = [&] {
+        int per_sm = 0, dev = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFlowThreads, 0) !=
+                cudaSuccess ||
+            cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            return 0ll;
+        }
+        return (long long)per_sm * sms;
+    }();
+    const int late = pdl_late(flow_blocks(fm.nf) <= resident) ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, f, fm, g, k, ctrl, kstep, partials, late);
 }
 
 template <class L, class M>

@@ -64,6 +64,20 @@ inline bool pdl_enabled() {
     return !(v && v[0] == '0');
 }
 
+// Where a single-solve step kernel lets the next step launch
+// (griddepcontrol.launch_dependents): after its own stores when its grid
+// fits in one resident wave -- the next step's blocks then arrive as this
+// one drains instead of sitting beside it (64^3: flow 4.60 -> 4.09 us per
+// iteration, transport 4.11 -> 3.66 us per step) -- and at its start when
+// it does not, so later waves overlap the next step's set-up.
+// PRT_PDL_LATE=all / none puts it at the end / the start for every grid.
+inline bool pdl_late(bool one_wave) {
+    const char* v = std::getenv("PRT_PDL_LATE");
+    if (v && v[0] == 'a') return true;
+    if (v && v[0] == 'n') return false;
+    return one_wave;
+}
+
 // Device-side state of FlowConvergence (prtlb_3d.py:168-252) for one solve.
 struct FlowCtrl {
     long long it_base;  // iterations completed before the current chunk
