@@ -315,10 +315,12 @@ class Batch(object):
         The host work of the solves collected by one wait (a finished flow
         solve's field and transport set-up, a finished run's snapshots) is
         done while the next graph replay runs, as in the served loop.
-        Between solves that finish, one launch runs up to 8 graph replays
-        (doubling while no solve finished), so the host's per-launch work
-        is paid less often; a solve that finishes is then seen at most 8
-        replays late, while the other solves keep advancing."""
+        One launch runs up to 8 graph replays (1, 2, 4, then 8), so the
+        host's per-launch work is paid less often and the host work of the
+        solves that finished has a long launch to hide behind; a solve that
+        finishes is seen at most 8 replays late (its place in the batch
+        costs nothing meanwhile), which for the longest solve of a batch
+        adds at most two such delays (its flow end, its transport end)."""
         out = []
         n = 0
         reps = 1
@@ -327,11 +329,9 @@ class Batch(object):
             if max_steps is not None:
                 steps = min(steps, max_steps - n)
             self.launch(steps)
-            quiet = not self._ready
             out.extend(self.process())
             self.wait(process=False)
-            quiet = quiet and not self._ready
-            reps = min(reps * 2, 8) if quiet else 1
+            reps = min(reps * 2, 8)
             n += steps
         out.extend(self.process())
         return out
