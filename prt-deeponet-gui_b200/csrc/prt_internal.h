@@ -78,6 +78,14 @@ inline bool pdl_late(bool one_wave) {
     return one_wave;
 }
 
+// The launch settings a captured loop graph bakes in (PRT_PDL, PRT_PDL_LATE),
+// as one number for the graph caches' keys.
+inline int pdl_key() {
+    const char* v = std::getenv("PRT_PDL_LATE");
+    const int late = (v && v[0] == 'a') ? 1 : (v && v[0] == 'n') ? 2 : 0;
+    return (pdl_enabled() ? 1 : 0) + 2 * late;
+}
+
 // Device-side state of FlowConvergence (prtlb_3d.py:168-252) for one solve.
 struct FlowCtrl {
     long long it_base;  // iterations completed before the current chunk

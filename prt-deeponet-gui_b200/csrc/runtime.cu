@@ -271,8 +271,7 @@ static int flow_graph(prt_ctx* ctx) {
     key.tol = p.tol; key.f = F.f.p;
     key.aux[0] = F.fluid.p; key.aux[1] = F.partials.p; key.aux[2] = F.ctrl.p;
     key.aux[3] = F.cells.p; key.aux[4] = (void*)F.fm.nbr; key.nf = F.nfluid;
-    const char* pdl = std::getenv("PRT_PDL");
-    key.pdl = (pdl && pdl[0] == '0') ? 0 : 1;
+    key.pdl = pdl_key();
     if (!F.graph.exec || !(key == F.key)) {
         CK(build_while_graph(ctx->stream,
                              F.graph, [&](cudaGraphConditionalHandle h, int use) {
@@ -720,7 +719,7 @@ static cudaError_t adr_emit(prt_ctx* ctx, cudaGraphConditionalHandle h, int use)
 static std::vector<unsigned char> adr_graph_key(prt_ctx* ctx) {
     AdrState& A = ctx->adr;
     const void* ptrs[3] = {A.means.p, A.src_slot.p, A.ctrl.p};
-    const int ints[2] = {A.rp.check, pdl_enabled() ? 1 : 0};
+    const int ints[2] = {A.rp.check, pdl_key()};
     std::vector<unsigned char> k(sizeof(AdrDev) + sizeof(prt_adr_params) + sizeof(ptrs) +
                                  sizeof(ints));
     unsigned char* q = k.data();

@@ -64,7 +64,7 @@ struct FlowKey {
     void* f = nullptr;
     void* aux[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     long long nf = -1;  // pore voxels: launch sizes and the lattice stride are baked in
-    int pdl = 0;        // step kernels captured with programmatic dependent launch
+    int pdl = 0;        // the launch settings the step kernels were captured with (pdl_key)
     bool operator==(const FlowKey& o) const {
         return nd == o.nd && precision == o.precision && every == o.every && g.nx == o.g.nx &&
                g.ny == o.g.ny && g.nz == o.g.nz && force == o.force && tau == o.tau &&

@@ -116,13 +116,16 @@ def test_buffers_kept_between_runs_hold_no_stale_values():
         ctx.close()
 
 
-@pytest.mark.parametrize("pdl", ["0", "1"])
-def test_transport_with_and_without_programmatic_launch(monkeypatch, pdl):
+@pytest.mark.parametrize("pdl,late", [("0", ""), ("1", ""), ("1", "all"), ("1", "none")])
+def test_transport_with_and_without_programmatic_launch(monkeypatch, pdl, late):
     """The transport step goes out with programmatic dependent launch by
     default (its voxel index, flags and face velocities are read while the
-    previous step drains) or plainly (PRT_PDL=0); both match the reference's
+    previous step drains) or plainly (PRT_PDL=0), letting the next step in at
+    its start or after its stores (PRT_PDL_LATE=none / all; by default after
+    the stores when its grid is one wave); every way matches the reference's
     golden runs bit for bit."""
     monkeypatch.setenv("PRT_PDL", pdl)
+    monkeypatch.setenv("PRT_PDL_LATE", late)
     for name in ("adr_spheres3d_biofilm", "adr_spheres3d_ns4", "adr_disks2d_first",
                  "adr_chan2d_capped"):
         z = load_golden(name)

@@ -136,19 +136,24 @@ def test_permeability_of_a_slit():
 
 def test_programmatic_dependent_launch_gives_the_same_field(monkeypatch):
     """The step kernels go out with programmatic dependent launch (the
-    default) or plainly (PRT_PDL=0): that changes when a kernel starts,
-    never what it computes.  The cached loop graph is keyed on the switch,
+    default) or plainly (PRT_PDL=0), and let the next step in at their start
+    or after their stores (PRT_PDL_LATE=none / all; by default after the
+    stores when the grid is one wave): that changes when a kernel starts,
+    never what it computes.  The cached loop graph is keyed on the switches,
     so each setting really runs its own launches."""
     from prtlb_gpu import sphere_pack_3d, stokes_d3q19
     g = sphere_pack_3d(24, 0.45, 0)
     out = {}
-    for mode in ("0", "1", "0"):
+    for mode, late in (("0", ""), ("1", ""), ("0", ""), ("1", "all"), ("1", "none")):
         monkeypatch.setenv("PRT_PDL", mode)
+        monkeypatch.setenv("PRT_PDL_LATE", late)
         with contextlib.redirect_stdout(io.StringIO()):
-            out.setdefault(mode, []).append(
+            out.setdefault(mode + late, []).append(
                 stokes_d3q19(g, nit=400, tol=1e-9, precision="fp32"))
     assert np.array_equal(out["1"][0], out["0"][0])
     assert np.array_equal(out["0"][1], out["0"][0])
+    assert np.array_equal(out["1all"][0], out["0"][0])
+    assert np.array_equal(out["1none"][0], out["0"][0])
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32", "fp16"])
