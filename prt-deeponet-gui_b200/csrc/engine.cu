@@ -14,6 +14,7 @@
 // it is rebuilt only when the set of classes, a grid size or a buffer
 // address changes.
 #include <cmath>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -644,12 +645,10 @@ extern "C" int prt_batch_add(prt_batch* b, prt_ctx* job) {
     // the count the job joins with (the batch advances it implicitly)
     BK(cudaSetDevice(job->device));
     long long c0 = 0;
-    if (job->flow_armed)
-        BK(cudaMemcpyAsync(&c0, &job->flow.ctrl.as<FlowCtrl>()->it_base, sizeof(c0),
-                           cudaMemcpyDeviceToHost, job->stream));
-    else
-        BK(cudaMemcpyAsync(&c0, &job->adr.ctrl.as<AdrCtrl>()->n_base, sizeof(c0),
-                           cudaMemcpyDeviceToHost, job->stream));
+    const char* src = job->flow_armed
+                          ? job->flow.ctrl.as<const char>() + offsetof(FlowCtrl, it_base)
+                          : job->adr.ctrl.as<const char>() + offsetof(AdrCtrl, n_base);
+    BK(cudaMemcpyAsync(&c0, src, sizeof(c0), cudaMemcpyDeviceToHost, job->stream));
     BK(cudaStreamSynchronize(job->stream));
     std::lock_guard<std::mutex> lk(b->mu);
     b->jobs.push_back(job);
