@@ -134,7 +134,8 @@ static cudaError_t launch_batch_t(const FlowJob* jobs, const BatchTile* tiles, c
     cfg.numAttrs = pdl_enabled() ? 1 : 0;
     // a batch step lets the next one in after its work whatever its grid:
     // its own pre-wait work is small (tile and descriptor), and 48 small
-    // solves ran 56.9k against 52.3k solves/h with the release at the start
+    // solves ran 56.9k solves/h with it against 52.3k with the release at
+    // the start (one run each)
     const int late = pdl_late(true) ? 1 : 0;
     if (uniform)
         return cudaLaunchKernelEx(&cfg, batch_flow_kernel<L, M, true>, jobs, tiles, ntiles, gstep,
