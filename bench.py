@@ -330,8 +330,12 @@ def run_ours(args, rank, world, torch, dist):
     if rank == 0 and not args.no_side:
         res["side"] = side_measurements(ctx, peak, kind)
         if world == 1:
-            res["side"]["batched_small_mix"] = batched_side(args, torch)
-            res["side"]["served_short"] = served_side(args, torch)
+            # figures beside the line: a failure there is recorded, not fatal
+            for key, fn in (("batched_small_mix", batched_side), ("served_short", served_side)):
+                try:
+                    res["side"][key] = fn(args, torch)
+                except Exception as e:  # noqa: BLE001
+                    res["side"][key] = {"error": "%s: %s" % (type(e).__name__, e)}
     ctx.close()
     return res
 
