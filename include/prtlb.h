@@ -348,7 +348,11 @@ const char* prt_batch_last_error(const prt_batch* b);
  * be used by other calls until it is collected or removed. */
 int prt_batch_add(prt_batch* b, prt_ctx* job);
 
-/* Takes a job out of the batch (not needed for collected jobs). */
+/* Takes a job out of the batch (not needed for collected jobs), between
+ * launches.  A batch keeps its jobs' iteration / step counts implicitly and
+ * writes them to a job's control block only on the steps that check or end
+ * it, so removing an unfinished job writes its count back; it can then join
+ * another batch (prt_batch_add) and go on from where it was. */
 int prt_batch_remove(prt_batch* b, prt_ctx* job);
 
 /* Enqueues `steps` batch steps and returns without waiting. */
